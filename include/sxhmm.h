@@ -1,0 +1,189 @@
+/*
+ * sxhmm — B200 hmmsearch engine, C ABI.
+ *
+ * Drop-in for the hmmsearch engine of raw-lab/sentinel-x (src/hmmer).  The
+ * boundary sits below `search_profiles` (src/hmmer/search.rs:213): parsing,
+ * profile configuration and reporting keep the reference's semantics on the
+ * host; the (profile x target) pair loop and the per-pair pipeline
+ * (`score_target`, src/hmmer/pipeline.rs:154) run on one NVIDIA B200.
+ *
+ * Conventions: every call returns SX_OK (0) or an SX_E* error class; the
+ * message of the last error on the calling thread is sx_last_error().  Inputs
+ * are borrowed for the duration of a call.  Objects returned through `out`
+ * pointers belong to the library until the matching *_free.  No call aborts or
+ * exits the process.  Calls on one engine are serialised by the engine.
+ */
+#ifndef SXHMM_H
+#define SXHMM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error classes ---------------------------------------------------- */
+#define SX_OK 0
+#define SX_EINVAL 1    /* bad argument / malformed input (e.g. a .hmm parse error)  */
+#define SX_ECUTOFF 2   /* GA/NC/TC cutoff requested but absent (search.rs:135-146)  */
+#define SX_ENOMEM 3    /* host or device allocation failed / admission refused     */
+#define SX_ECUDA 4     /* CUDA runtime error                                        */
+#define SX_ETIMEOUT 5  /* a bounded device wait gave up                             */
+#define SX_EIO 6       /* file could not be opened or read                          */
+
+/* Cutoff kinds (hmmsearch -E/--domE, -T/--domT, --cut_ga/nc/tc;
+ * src/hmmer/search.rs:26-38). */
+#define SX_CUT_EVALUE 0
+#define SX_CUT_BITS 1
+#define SX_CUT_GA 2
+#define SX_CUT_NC 3
+#define SX_CUT_TC 4
+
+/* Engine options. */
+#define SX_FLAG_PLAIN 1u /* run the plain one-pair-per-block kernels instead of the batched cascade */
+
+typedef struct sx_engine sx_engine;
+typedef struct sx_profiles sx_profiles;
+typedef struct sx_targets sx_targets;
+typedef struct sx_hits sx_hits;
+
+typedef struct {
+  int32_t device;       /* CUDA device ordinal                                       */
+  int32_t host_threads; /* host threads for domain definition; 0 = all cores         */
+  uint32_t flags;       /* SX_FLAG_*                                                 */
+  int32_t reserved;
+  int64_t batch_bytes;  /* device bytes per streamed batch; 0 = 2 GiB                */
+} sx_opts;
+
+/* PipelineConfig + SearchConfig (src/hmmer/pipeline.rs:27-42,
+ * src/hmmer/search.rs:42-47).  z = NaN means "number of targets". */
+typedef struct {
+  int32_t cutoff_kind;  /* SX_CUT_* */
+  int32_t filters;      /* 0 = hmmsearch --max */
+  int32_t null2;        /* 0 = --nonull2 */
+  int32_t reserved;
+  double seq_threshold; /* E-value or bits, per cutoff_kind (ignored for GA/NC/TC) */
+  double dom_threshold;
+  double f1, f2, f3;
+  double z;
+} sx_search_cfg;
+
+/* One reported target: `Hit` (src/hmmer/search.rs:101-116). */
+typedef struct {
+  int32_t profile_index; /* index in the sx_profiles set */
+  int32_t target_index;  /* index in the sx_targets set  */
+  int32_t qlen, tlen;
+  float score, bias;
+  double evalue;
+  float nexpected;
+  int32_t ndomains;
+  int32_t domain_offset; /* first domain in sx_hits_domains() */
+  int32_t reserved;
+} sx_hit;
+
+/* One domain: `DomainHit` (src/hmmer/search.rs:84-97). */
+typedef struct {
+  float score, bias;
+  double c_evalue, i_evalue;
+  int32_t hmm_from, hmm_to, ali_from, ali_to, env_from, env_to;
+  int32_t reported;
+  int32_t reserved;
+} sx_domain;
+
+/* Header of one profile: name, accession, M, cutoffs and STATS
+ * (src/hmmer/model.rs:53-71). Missing values are NaN; strings live as long
+ * as the sx_profiles set. */
+typedef struct {
+  const char* name;
+  const char* acc;  /* NULL if absent */
+  const char* desc; /* NULL if absent */
+  int32_t m;
+  int32_t calibrated;
+  float ga[2], tc[2], nc[2];
+  double msv[2], viterbi[2], forward[2]; /* (mu|tau, lambda) */
+} sx_profile_info;
+
+/* ---- engine ------------------------------------------------------------ */
+/* New: one engine per device. */
+int sx_create(const sx_opts* opts, sx_engine** out);
+void sx_destroy(sx_engine* e);
+/* Message of the last error on this thread ("" if none). */
+const char* sx_last_error(void);
+
+/* ---- profiles ---------------------------------------------------------- */
+/* Replaces open_hmm + HmmReader + Hmm::configure (src/hmmer/parse.rs:42-236,
+ * src/hmmer/model.rs:146-245): parses a HMMER3/b..f file (gzip detected by
+ * magic bytes), configures every profile and uploads it to the device. */
+int sx_profiles_load_file(sx_engine* e, const char* path, sx_profiles** out);
+/* Same from an in-memory HMMER3 text; `source` names it in error messages. */
+int sx_profiles_load_text(sx_engine* e, const char* text, size_t len, const char* source, sx_profiles** out);
+int32_t sx_profiles_count(const sx_profiles* p);
+int sx_profiles_info(const sx_profiles* p, int32_t i, sx_profile_info* out);
+void sx_profiles_free(sx_profiles* p);
+
+/* ---- targets ----------------------------------------------------------- */
+/* Replaces Targets::new (src/hmmer/search.rs:56-67): digitises ASCII protein
+ * sequences (src/hmmer/alphabet.rs:58-93) and uploads them.  ids may be NULL. */
+int sx_targets_create(sx_engine* e, const char* const* ids, const uint8_t* const* seqs, const size_t* lens, size_t n,
+                      sx_targets** out);
+/* Already-digitised residues (codes 0..24) packed back to back: target i is
+ * dsq[offsets[i] .. offsets[i]+lens[i]). */
+int sx_targets_create_digital(sx_engine* e, const uint8_t* dsq, const int64_t* offsets, const int64_t* lens, size_t n,
+                              sx_targets** out);
+int64_t sx_targets_count(const sx_targets* t);
+void sx_targets_free(sx_targets* t);
+
+/* ---- search ------------------------------------------------------------ */
+/* Replaces search_profiles (src/hmmer/search.rs:213-234): every profile x
+ * every target through MSV -> bias -> Viterbi -> Forward filters, Backward,
+ * posterior domain definition, envelope rescoring, null2 and reporting.  Hits
+ * come out in profile order, then target order, like the reference. */
+int sx_search(sx_engine* e, const sx_profiles* p, const sx_targets* t, const sx_search_cfg* cfg, sx_hits** out);
+size_t sx_hits_count(const sx_hits* h);
+const sx_hit* sx_hits_array(const sx_hits* h);
+size_t sx_hits_domain_count(const sx_hits* h);
+const sx_domain* sx_hits_domains(const sx_hits* h);
+void sx_hits_free(sx_hits* h);
+
+/* Per-stage counters of the last sx_search on this engine: pairs entering and
+ * leaving each stage, DP cells per stage and device milliseconds per stage.
+ * stage: 0 MSV, 1 bias, 2 Viterbi, 3 Forward pre-screen, 4 Forward/Backward
+ * rows, 5 host domain definition. */
+typedef struct {
+  int64_t pairs_in[6], pairs_out[6];
+  double cells[6];
+  double ms[6];
+  int64_t kernel_launches;
+} sx_search_stats;
+int sx_last_search_stats(const sx_engine* e, sx_search_stats* out);
+
+/* ---- stage scores for explicit pairs ----------------------------------- */
+/* Scores of msv (dp.rs:69), viterbi_score (dp.rs:152), forward (dp.rs:229),
+ * backward (dp.rs:301) and bias_filter_score (pipeline.rs:107) for each pair
+ * (pair_profile[i], pair_target[i]), target-length configured and multihit
+ * as in score_target.  Any output pointer may be NULL to skip that stage. */
+int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, const int32_t* pair_profile,
+                   const int32_t* pair_target, size_t npairs, float* msv, float* viterbi, float* forward,
+                   float* backward, float* bias);
+
+/* ---- adjoint ----------------------------------------------------------- */
+/* Gradient of each pair's Forward log score lnZ (multihit, target-length
+ * config; dp.rs:229-298) with respect to the profile's log-space scores:
+ *   d_msc [npairs][25][M+1]  match emission scores msc[x][k]
+ *   d_isc [npairs][25][M+1]  insert emission scores (0 in the model)
+ *   d_trans[npairs][8][M+1]  transitions MM MI MD IM II DM DD of source node k,
+ *                            then the local entry B->M_k
+ * i.e. the posterior expected counts of each emission and transition (the
+ * quantities decode(), dp.rs:1278-1306, sums for domain definition).  All
+ * pairs must use profiles of one length M (= m).  lnz[npairs] receives lnZ.
+ * The Forward pass keeps sqrt(L) checkpoint rows and Backward recomputes the
+ * rows between checkpoints, so device scratch is O(M sqrt(L)) per pair. */
+int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, const int32_t* pair_profile,
+                      const int32_t* pair_target, size_t npairs, int32_t m, float* d_msc, float* d_isc,
+                      float* d_trans, double* lnz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SXHMM_H */

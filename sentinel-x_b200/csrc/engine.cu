@@ -1,0 +1,1238 @@
+// sxhmm engine: device data layout, the batched hmmsearch cascade on one
+// B200, and the C ABI declared in include/sxhmm.h.
+//
+// Flow of sx_search (replaces the rayon pair loop of search_profiles,
+// src/hmmer/search.rs:213-234, and score_target, src/hmmer/pipeline.rs:154):
+//   1. MSV over every (profile, target) pair: CTA tiles of (profile, slice of
+//      the length-sorted targets); exact F1 decision; survivors appended to
+//      per-shape lists.
+//   2. composition-bias filter, 3. Viterbi, 4. Forward score: each a
+//      pair-list kernel over the previous stage's survivors; decisions that
+//      involve a device logarithm are taken with a small slack so the device
+//      never rejects a pair the reference keeps.
+//   5. host: exact re-check of every decision with the reference's libm;
+//      device Forward/Backward passes that emit the raw special rows of the
+//      final pairs (chunked); host posterior domain definition, envelope
+//      rescoring and reporting on a thread pool.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/sxhmm.h"
+#include "internal.hpp"
+#include "kernels.cuh"
+
+using namespace sx;
+using sxk::BinRegion;
+using sxk::DevProfile;
+using sxk::MsvTile;
+using sxk::PairRec;
+using sxk::Thresholds;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+struct CudaError {
+  int code;
+  std::string msg;
+};
+
+#define CK(call)                                                                                      \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
+    if (e_ != cudaSuccess)                                                                            \
+      throw CudaError{e_ == cudaErrorMemoryAllocation ? SX_ENOMEM : SX_ECUDA,                         \
+                      std::string(#call) + ": " + cudaGetErrorString(e_)};                            \
+  } while (0)
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {  // grow-only, contents undefined
+    if (count <= n && p) return;
+    release();
+    CK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    n = std::max<size_t>(count, 1);
+  }
+  void upload(const T* src, size_t count, cudaStream_t s) {
+    alloc(count);
+    if (count) CK(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+};
+
+// ---- kernel shapes ---------------------------------------------------------
+// MSV (G lanes per target, C columns per lane) shapes compiled into the library.
+struct MsvShape {
+  int g, c;
+};
+constexpr MsvShape kMsvShapes[] = {{1, 8},  {1, 16},  {1, 24},  {1, 32},  {2, 8},   {2, 16},  {2, 24},
+                                   {2, 32}, {4, 8},   {4, 16},  {4, 24},  {4, 32},  {8, 8},   {8, 16},
+                                   {8, 24}, {8, 32},  {16, 8},  {16, 16}, {16, 24}, {16, 32}, {32, 8},
+                                   {32, 16}, {32, 24}, {32, 32}, {32, 48}, {32, 64}};
+constexpr int kNumMsvShapes = sizeof(kMsvShapes) / sizeof(kMsvShapes[0]);
+constexpr int kMaxM = 2048;
+// Warp-chunked column counts (columns per lane, 32 lanes per pair).
+constexpr int kVcBins[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64};
+constexpr int kNumVbins = sizeof(kVcBins) / sizeof(kVcBins[0]);
+
+typedef void (*MsvFn)(const MsvTile*, const DevProfile*, const Thresholds*, const float4*, const uint8_t*,
+                      const int64_t*, const int32_t*, const float4*, const int32_t*, float*, const int32_t*, PairRec*,
+                      const BinRegion*, unsigned*, unsigned*);
+typedef void (*VitFn)(const PairRec*, const unsigned*, const BinRegion*, int, PairRec*, const BinRegion*, unsigned*,
+                      unsigned*, const DevProfile*, const Thresholds*, const float*, const uint8_t*, const int64_t*,
+                      const int32_t*, const float4*, float, float*);
+typedef void (*FwdFn)(const PairRec*, const unsigned*, const BinRegion*, int, PairRec*, const BinRegion*, unsigned*,
+                      unsigned*, const DevProfile*, const Thresholds*, const float*, const uint8_t*, const int64_t*,
+                      const int32_t*, const float4*, float, float*, const int64_t*);
+typedef void (*BwdFn)(const PairRec*, const unsigned*, const BinRegion*, int, const DevProfile*, const float*,
+                      const uint8_t*, const int64_t*, const int32_t*, const float4*, float*, const int64_t*);
+
+template <int I>
+struct MsvTable {
+  static void fill(MsvFn* t) {
+    t[I] = sxk::msv_kernel<kMsvShapes[I].g, kMsvShapes[I].c>;
+    MsvTable<I + 1>::fill(t);
+  }
+};
+template <>
+struct MsvTable<kNumMsvShapes> {
+  static void fill(MsvFn*) {}
+};
+template <int I>
+struct VbinTable {
+  static void fill(VitFn* v, FwdFn* f, BwdFn* b) {
+    v[I] = sxk::viterbi_kernel<kVcBins[I]>;
+    f[I] = sxk::forward_kernel<kVcBins[I]>;
+    b[I] = sxk::backward_kernel<kVcBins[I]>;
+    VbinTable<I + 1>::fill(v, f, b);
+  }
+};
+template <>
+struct VbinTable<kNumVbins> {
+  static void fill(VitFn*, FwdFn*, BwdFn*) {}
+};
+
+struct KernelTables {
+  MsvFn msv[kNumMsvShapes];
+  VitFn vit[kNumVbins];
+  FwdFn fwd[kNumVbins];
+  BwdFn bwd[kNumVbins];
+  KernelTables() {
+    MsvTable<0>::fill(msv);
+    VbinTable<0>::fill(vit, fwd, bwd);
+  }
+};
+const KernelTables& kernels() {
+  static KernelTables t;
+  return t;
+}
+
+// Pick the MSV shape with the fewest estimated issued instructions per useful
+// DP cell: per row a warp issues ~(2.6C + 2log2(G) + 17) instructions and
+// advances 32/G targets by M cells each.
+int choose_msv_shape(int m) {
+  int best = -1;
+  double best_cost = 1e30;
+  for (int s = 0; s < kNumMsvShapes; s++) {
+    const int g = kMsvShapes[s].g, c = kMsvShapes[s].c;
+    if (g * c < m) continue;
+    const double instr = 2.6 * c + 2.0 * std::log2((double)g) + 17.0;
+    const double cost = instr / ((32.0 / g) * m);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = s;
+    }
+  }
+  return best;
+}
+int choose_vbin(int m) {
+  const int need = (m + 31) / 32;
+  for (int b = 0; b < kNumVbins; b++)
+    if (kVcBins[b] >= need) return b;
+  return -1;
+}
+
+// ---- thread pool helper ----------------------------------------------------
+template <typename F>
+void parallel_for(size_t n, int nthreads, F&& f) {
+  if (n == 0) return;
+  const int nt = std::max(1, std::min<int>(nthreads, (int)n));
+  std::atomic<size_t> next{0};
+  auto work = [&]() {
+    for (;;) {
+      const size_t i = next.fetch_add(1);
+      if (i >= n) break;
+      f(i);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; t++) th.emplace_back(work);
+  work();
+  for (auto& t : th) t.join();
+}
+
+// Smallest f32 statistic s with pass(s) true, assuming pass is monotone
+// (false below the boundary, true above); +inf if it never passes, -inf if it
+// always passes on the finite range.
+template <typename Pred>
+float f32_boundary(Pred pass) {
+  auto key = [](float f) {
+    int32_t i;
+    memcpy(&i, &f, 4);
+    return i >= 0 ? i : (int32_t)(0x80000000u - (uint32_t)i) * -1;  // monotone int order
+  };
+  (void)key;
+  // order-preserving map float <-> int64 over finite floats
+  auto to_ord = [](float f) -> int64_t {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return (u & 0x80000000u) ? -(int64_t)(u & 0x7fffffffu) : (int64_t)u;
+  };
+  auto from_ord = [](int64_t o) -> float {
+    uint32_t u = o < 0 ? (0x80000000u | (uint32_t)(-o)) : (uint32_t)o;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+  };
+  int64_t lo = to_ord(-3.0e38f), hi = to_ord(3.0e38f);
+  if (pass(from_ord(lo))) return -INFINITY;
+  if (!pass(from_ord(hi))) return INFINITY;
+  while (hi - lo > 1) {  // invariant: !pass(lo), pass(hi)
+    const int64_t mid = lo + (hi - lo) / 2;
+    if (pass(from_ord(mid))) hi = mid;
+    else lo = mid;
+  }
+  return from_ord(hi);
+}
+
+}  // namespace
+
+// ---- engine objects ----------------------------------------------------------
+struct sx_engine {
+  int device = 0;
+  int host_threads = 1;
+  uint32_t flags = 0;
+  int64_t batch_bytes = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[8] = {};
+  std::mutex mu;
+  sx_search_stats stats{};
+  // grow-only device scratch
+  DevBuf<PairRec> lists[4];
+  DevBuf<BinRegion> bins[4];
+  DevBuf<unsigned> counts;   // 4 stages x kNumVbins
+  DevBuf<unsigned> overflow;
+  DevBuf<MsvTile> tiles;
+  DevBuf<Thresholds> thr;
+  DevBuf<float> rows_f, rows_b;
+  DevBuf<int64_t> row_off;
+  DevBuf<float> scores;
+  DevBuf<int32_t> slots, plist;
+};
+
+struct sx_profiles {
+  sx_engine* eng = nullptr;
+  std::vector<ProfileHost> h;
+  std::vector<DevProfile> dp;
+  std::vector<int> msv_shape;
+  DevBuf<DevProfile> d_prof;
+  DevBuf<float4> d_msv;
+  DevBuf<float> d_vfb;
+  DevBuf<double> d_bias;
+};
+
+struct sx_targets {
+  sx_engine* eng = nullptr;
+  std::vector<std::string> ids;
+  std::vector<uint8_t> dsq;  // packed digital residues, each target 16-byte aligned
+  std::vector<int64_t> off;
+  std::vector<int32_t> len;
+  std::vector<int32_t> order;  // indices sorted by length, longest first
+  double residues = 0;
+  DevBuf<uint8_t> d_res;
+  DevBuf<int64_t> d_off;
+  DevBuf<int32_t> d_len;
+  DevBuf<float4> d_tpar;  // MSV tloop, tmove, null score
+  DevBuf<float4> d_xsc;   // multihit loop, move (log), loop, move (prob)
+  DevBuf<int32_t> d_order;
+};
+
+struct sx_hits {
+  std::vector<sx_hit> hits;
+  std::vector<sx_domain> doms;
+};
+
+namespace {
+
+// ---- profile packing --------------------------------------------------------
+void pack_profiles(sx_profiles* P) {
+  const size_t np = P->h.size();
+  P->dp.resize(np);
+  P->msv_shape.resize(np);
+  int64_t msv_total = 0, vfb_total = 0;
+  for (size_t i = 0; i < np; i++) {
+    const ProfileHost& h = P->h[i];
+    DevProfile& d = P->dp[i];
+    memset(&d, 0, sizeof d);
+    d.m = h.m;
+    const int s = choose_msv_shape(h.m);
+    const int vb = choose_vbin(h.m);
+    if (s < 0 || vb < 0)
+      throw CudaError{SX_EINVAL, "profile '" + h.name + "' has M=" + std::to_string(h.m) +
+                                     " nodes; this build supports M <= " + std::to_string(kMaxM)};
+    P->msv_shape[i] = s;
+    d.msv_g = kMsvShapes[s].g;
+    d.msv_c = kMsvShapes[s].c;
+    d.vbin = vb;
+    d.vc = kVcBins[vb];
+    d.msv_off = msv_total;
+    msv_total += 25LL * (d.msv_c / 4) * d.msv_g;
+    d.vfb_off = vfb_total;
+    vfb_total += (int64_t)sxk::kImgRows * 32 * d.vc;
+    d.msv_tbm = h.msv_tbm;
+  }
+  std::vector<float4> msv((size_t)msv_total);
+  std::vector<float> vfb((size_t)vfb_total);
+  std::vector<double> bias(np * 54);
+  for (size_t i = 0; i < np; i++) {
+    const ProfileHost& h = P->h[i];
+    const DevProfile& d = P->dp[i];
+    const int m = h.m;
+    // MSV image: residue row x, float4 chunk c4 of lane j at (x*NC4 + c4)*G + j;
+    // lane j's column c is k = j*C + c + 1.
+    {
+      const int G = d.msv_g, C = d.msv_c, NC4 = C / 4;
+      float4* base = msv.data() + d.msv_off;
+      for (int x = 0; x < 25; x++)
+        for (int j = 0; j < G; j++)
+          for (int c4 = 0; c4 < NC4; c4++) {
+            float v[4];
+            for (int e = 0; e < 4; e++) {
+              const int k = j * C + c4 * 4 + e + 1;
+              v[e] = k <= m ? h.msc_row(x)[k] : kNegInf;
+            }
+            base[((size_t)x * NC4 + c4) * G + j] = make_float4(v[0], v[1], v[2], v[3]);
+          }
+    }
+    // warp-chunked image: row r, lane l, column c (k = l*vc + c + 1) at (r*vc + c)*32 + l
+    {
+      const int vc = d.vc;
+      float* base = vfb.data() + d.vfb_off;
+      auto put = [&](int r, const std::function<float(int)>& f, float pad) {
+        for (int l = 0; l < 32; l++)
+          for (int c = 0; c < vc; c++) {
+            const int k = l * vc + c + 1;
+            base[((size_t)r * vc + c) * 32 + l] = k <= m ? f(k) : pad;
+          }
+      };
+      for (int x = 0; x < 25; x++) {
+        put(sxk::kRowMsc + x, [&](int k) { return h.msc_row(x)[k]; }, kNegInf);
+        put(sxk::kRowMo + x, [&](int k) { return h.mo_row(x)[k]; }, 0.0f);
+      }
+      const auto& t = h.t;
+      const auto& p = h.p;
+      auto shl = [&](const std::vector<float>& v) { return [&v](int k) { return v[k - 1]; }; };
+      auto at = [&](const std::vector<float>& v) { return [&v](int k) { return v[k]; }; };
+      put(sxk::kRowVit + 0, shl(t[TMM]), kNegInf);
+      put(sxk::kRowVit + 1, shl(t[TIM]), kNegInf);
+      put(sxk::kRowVit + 2, shl(t[TDM]), kNegInf);
+      put(sxk::kRowVit + 3, at(t[TBM]), kNegInf);
+      put(sxk::kRowVit + 4, at(t[TMI]), kNegInf);
+      put(sxk::kRowVit + 5, at(t[TII]), kNegInf);
+      put(sxk::kRowVit + 6, shl(t[TMD]), kNegInf);
+      put(sxk::kRowVit + 7, shl(t[TDD]), kNegInf);
+      put(sxk::kRowFwd + 0, at(p[TBM]), 0.0f);
+      put(sxk::kRowFwd + 1, shl(p[TMM]), 0.0f);
+      put(sxk::kRowFwd + 2, shl(p[TIM]), 0.0f);
+      put(sxk::kRowFwd + 3, shl(p[TDM]), 0.0f);
+      put(sxk::kRowFwd + 4, at(p[TMI]), 0.0f);
+      put(sxk::kRowFwd + 5, at(p[TII]), 0.0f);
+      put(sxk::kRowFwd + 6, shl(p[TMD]), 0.0f);
+      put(sxk::kRowFwd + 7, shl(p[TDD]), 0.0f);
+      put(sxk::kRowBwd + 0, at(p[TMM]), 0.0f);
+      put(sxk::kRowBwd + 1, at(p[TMI]), 0.0f);
+      put(sxk::kRowBwd + 2, at(p[TMD]), 0.0f);
+      put(sxk::kRowBwd + 3, at(p[TIM]), 0.0f);
+      put(sxk::kRowBwd + 4, at(p[TII]), 0.0f);
+      put(sxk::kRowBwd + 5, at(p[TDM]), 0.0f);
+      put(sxk::kRowBwd + 6, at(p[TDD]), 0.0f);
+      put(sxk::kRowBwd + 7, at(p[TBM]), 0.0f);
+    }
+    // composition-bias filter table (src/hmmer/pipeline.rs:110-131)
+    {
+      double* b = bias.data() + i * 54;
+      for (int x = 0; x < 25; x++) b[x] = b[25 + x] = 1.0;
+      for (int x = 0; x < NRES; x++) b[25 + x] = (double)h.compo[x] / (double)kBackground[x];
+      for (int code = 20; code <= 23; code++) {
+        const Degenerate& dg = degenerate(code);
+        double e0 = 0, e1 = 0, z = 0;
+        for (int q = 0; q < dg.n; q++) {
+          e0 += (double)kBackground[dg.members[q]];
+          e1 += (double)h.compo[dg.members[q]];
+          z += (double)kBackground[dg.members[q]];
+        }
+        b[code] = e0 / z;
+        b[25 + code] = e1 / z;
+      }
+      const double l0 = 400.0, l1 = (double)m / 8.0;
+      b[50] = l0 / (l0 + 1.0);
+      b[51] = 1.0 / (l0 + 1.0);
+      b[52] = 1.0 / (l1 + 1.0);
+      b[53] = l1 / (l1 + 1.0);
+    }
+  }
+  cudaStream_t s = P->eng->stream;
+  P->d_prof.upload(P->dp.data(), np, s);
+  P->d_msv.upload(msv.data(), msv.size(), s);
+  P->d_vfb.upload(vfb.data(), vfb.size(), s);
+  P->d_bias.upload(bias.data(), bias.size(), s);
+  CK(cudaStreamSynchronize(s));
+}
+
+// ---- target packing ---------------------------------------------------------
+void pack_targets(sx_targets* T) {
+  const size_t n = T->len.size();
+  std::vector<float4> tpar(n), xsc(n);
+  T->residues = 0;
+  for (size_t i = 0; i < n; i++) {
+    const int64_t l = T->len[i];
+    const float lf = (float)l;
+    // MSV length model (src/hmmer/dp.rs:98-100) and the multihit Xsc (model.rs:284-312)
+    const float tloop = std::log(lf / (lf + 3.0f));
+    const float tmove = std::log(3.0f / (lf + 3.0f));
+    tpar[i] = make_float4(tloop, tmove, null1_score(l), 0.0f);
+    const SpecialTr st = special_transitions(l, true);
+    xsc[i] = make_float4(st.loop, st.move, st.ploop, st.pmove);
+    T->residues += (double)l;
+  }
+  T->order.resize(n);
+  std::iota(T->order.begin(), T->order.end(), 0);
+  std::stable_sort(T->order.begin(), T->order.end(), [&](int a, int b) { return T->len[a] > T->len[b]; });
+  cudaStream_t s = T->eng->stream;
+  T->d_res.upload(T->dsq.data(), T->dsq.size(), s);
+  T->d_off.upload(T->off.data(), n, s);
+  T->d_len.upload(T->len.data(), n, s);
+  T->d_tpar.upload(tpar.data(), n, s);
+  T->d_xsc.upload(xsc.data(), n, s);
+  T->d_order.upload(T->order.data(), n, s);
+  CK(cudaStreamSynchronize(s));
+}
+
+void append_target(sx_targets* T, const uint8_t* dig, size_t l) {
+  const int64_t o = (int64_t)T->dsq.size();
+  T->off.push_back(o);
+  T->len.push_back((int32_t)l);
+  T->dsq.insert(T->dsq.end(), dig, dig + l);
+  // pad to a 16-byte boundary; kernels read up to 48 bytes past a target
+  size_t padded = (T->dsq.size() + 15) & ~(size_t)15;
+  T->dsq.resize(padded, SYM_STAR);
+}
+
+// ---- thresholds ---------------------------------------------------------------
+// Per profile, the smallest f32 bit statistic that passes each filter
+// (pipeline.rs:164-183).  The tails are monotone in the statistic, except the
+// Gumbel survival around its branch at 1e-5; a threshold within 2% of that
+// point disables device filtering for the stage (the host still decides).
+std::vector<Thresholds> make_thresholds(const std::vector<ProfileHost>& H, const SearchOpts& o) {
+  std::vector<Thresholds> th(H.size());
+  auto near_branch = [](double f) { return f > 0.98e-5 && f < 1.02e-5; };
+  for (size_t i = 0; i < H.size(); i++) {
+    const ProfileHost& h = H[i];
+    Thresholds& t = th[i];
+    if (!o.filters || !h.calibrated()) {
+      t.s1 = t.s2 = t.s3 = -INFINITY;
+      t.exact = 0;
+      continue;
+    }
+    t.exact = 1;
+    const double mmu = h.msv[0], mlam = h.msv[1], vmu = h.vit[0], vlam = h.vit[1], ftau = h.fwd[0], flam = h.fwd[1];
+    t.s1 = near_branch(o.f1) ? -INFINITY : f32_boundary([&](float s) { return !(gumbel_survival((double)s, mmu, mlam) > o.f1); });
+    t.s2 = near_branch(o.f2) ? -INFINITY : f32_boundary([&](float s) { return !(gumbel_survival((double)s, vmu, vlam) > o.f2); });
+    t.s3 = f32_boundary([&](float s) { return !(std::exp(exp_tail_logsurv((double)s, ftau, flam)) > o.f3); });
+    if (std::isnan(t.s1)) t.s1 = -INFINITY;
+    if (std::isnan(t.s2)) t.s2 = -INFINITY;
+    if (std::isnan(t.s3)) t.s3 = -INFINITY;
+  }
+  return th;
+}
+
+constexpr float kSlackBits = 1.0e-3f;  // device-log decisions: never reject what the reference keeps
+
+struct StageLists {
+  std::vector<BinRegion> reg;
+  int64_t total = 0;
+};
+
+StageLists make_regions(const std::vector<double>& want) {
+  StageLists s;
+  s.reg.resize(kNumVbins);
+  int64_t off = 0;
+  for (int b = 0; b < kNumVbins; b++) {
+    const uint32_t cap = (uint32_t)std::min<double>(std::max(want[b], 0.0), 4.0e9);
+    s.reg[b].off = off;
+    s.reg[b].cap = cap;
+    s.reg[b].pad = 0;
+    off += cap;
+  }
+  s.total = off;
+  return s;
+}
+
+struct FinalPair {
+  int32_t p, t;
+  float usc, filtersc, vsc;
+  int32_t slot;
+};
+
+// Device Forward and Backward with row output for `pairs`, in chunks bounded
+// by `row_budget` floats per direction; calls sink(i, fwd_rows, bwd_rows).
+template <typename Sink>
+void rows_pass(sx_engine* E, const sx_profiles* P, const sx_targets* T, const std::vector<FinalPair>& pairs,
+               Sink&& sink) {
+  if (pairs.empty()) return;
+  const auto& K = kernels();
+  const int64_t row_budget = std::max<int64_t>(E->batch_bytes / 2 / (int64_t)sizeof(float), 1 << 20);
+  size_t i0 = 0;
+  while (i0 < pairs.size()) {
+    // chunk [i0, i1)
+    size_t i1 = i0;
+    int64_t used = 0;
+    while (i1 < pairs.size()) {
+      const int64_t need = 6 * ((int64_t)T->len[pairs[i1].t] + 1);
+      if (i1 > i0 && used + need > row_budget) break;
+      used += need;
+      i1++;
+    }
+    // group by vbin, assign row offsets
+    std::vector<std::vector<size_t>> byb(kNumVbins);
+    for (size_t i = i0; i < i1; i++) byb[P->dp[pairs[i].p].vbin].push_back(i);
+    std::vector<PairRec> recs;
+    std::vector<int64_t> roff;
+    std::vector<BinRegion> reg(kNumVbins);
+    std::vector<unsigned> cnt(kNumVbins, 0);
+    std::vector<size_t> which;
+    int64_t ro = 0;
+    for (int b = 0; b < kNumVbins; b++) {
+      reg[b].off = (int64_t)recs.size();
+      reg[b].cap = (uint32_t)byb[b].size();
+      reg[b].pad = 0;
+      cnt[b] = (unsigned)byb[b].size();
+      for (size_t i : byb[b]) {
+        const FinalPair& f = pairs[i];
+        PairRec r{f.p, f.t, f.usc, f.filtersc, f.vsc, 0.f, f.slot, 0};
+        recs.push_back(r);
+        roff.push_back(ro);
+        which.push_back(i);
+        ro += 6 * ((int64_t)T->len[f.t] + 1);
+      }
+    }
+    cudaStream_t s = E->stream;
+    E->lists[3].upload(recs.data(), recs.size(), s);
+    E->row_off.upload(roff.data(), roff.size(), s);
+    E->bins[3].upload(reg.data(), reg.size(), s);
+    E->counts.alloc(4 * kNumVbins);
+    CK(cudaMemcpyAsync(E->counts.p + 3 * kNumVbins, cnt.data(), sizeof(unsigned) * kNumVbins, cudaMemcpyHostToDevice, s));
+    E->rows_f.alloc((size_t)ro);
+    E->rows_b.alloc((size_t)ro);
+    // rows the kernels never touch are zero
+    CK(cudaMemsetAsync(E->rows_f.p, 0, sizeof(float) * (size_t)ro, s));
+    CK(cudaMemsetAsync(E->rows_b.p, 0, sizeof(float) * (size_t)ro, s));
+    for (int b = 0; b < kNumVbins; b++) {
+      if (!cnt[b]) continue;
+      const int blocks = (int)std::min<int64_t>((cnt[b] + 7) / 8, (int64_t)E->num_sms * 16);
+      K.fwd[b]<<<blocks, 256, 0, s>>>(E->lists[3].p, E->counts.p + 3 * kNumVbins, E->bins[3].p, b, nullptr, nullptr,
+                                      nullptr, E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p,
+                                      T->d_off.p, T->d_len.p, T->d_xsc.p, 0.f, E->rows_f.p, E->row_off.p);
+      K.bwd[b]<<<blocks, 256, 0, s>>>(E->lists[3].p, E->counts.p + 3 * kNumVbins, E->bins[3].p, b, P->d_prof.p,
+                                      P->d_vfb.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p, E->rows_b.p,
+                                      E->row_off.p);
+      E->stats.kernel_launches += 2;
+    }
+    CK(cudaGetLastError());
+    std::vector<float> hf((size_t)ro), hb((size_t)ro);
+    CK(cudaMemcpyAsync(hf.data(), E->rows_f.p, sizeof(float) * (size_t)ro, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hb.data(), E->rows_b.p, sizeof(float) * (size_t)ro, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    parallel_for(which.size(), E->host_threads, [&](size_t q) {
+      sink(which[q], hf.data() + roff[q], hb.data() + roff[q]);
+    });
+    i0 = i1;
+  }
+}
+
+struct PairResult {
+  bool hit = false;
+  HitOut h;
+};
+
+// search.rs:131-210: thresholds, E-values, domain c-/i-E-values, reported flags.
+int report(const sx_profiles* P, const sx_targets* T, const sx_search_cfg* cfg,
+           std::vector<std::vector<std::pair<int32_t, HitOut>>>& per_profile, sx_hits* out) {
+  const double z = std::max(std::isnan(cfg->z) ? (double)T->len.size() : cfg->z, 1.0);
+  for (size_t pi = 0; pi < P->h.size(); pi++) {
+    const ProfileHost& h = P->h[pi];
+    bool is_e = false;
+    double e_seq = 0, e_dom = 0;
+    float t_seq = 0, t_dom = 0;
+    switch (cfg->cutoff_kind) {
+      case SX_CUT_EVALUE: is_e = true; e_seq = cfg->seq_threshold; e_dom = cfg->dom_threshold; break;
+      case SX_CUT_BITS: t_seq = (float)cfg->seq_threshold; t_dom = (float)cfg->dom_threshold; break;
+      case SX_CUT_GA: t_seq = h.ga[0]; t_dom = h.ga[1]; break;
+      case SX_CUT_NC: t_seq = h.nc[0]; t_dom = h.nc[1]; break;
+      case SX_CUT_TC: t_seq = h.tc[0]; t_dom = h.tc[1]; break;
+    }
+    auto& raws = per_profile[pi];
+    std::sort(raws.begin(), raws.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    const size_t first_hit = out->hits.size();
+    for (auto& [ti, r] : raws) {
+      const double evalue = std::exp(r.lnp) * z;
+      const bool keep = is_e ? (evalue <= e_seq) : (r.bits >= t_seq);
+      if (!keep) continue;
+      sx_hit hh{};
+      hh.profile_index = (int32_t)pi;
+      hh.target_index = ti;
+      hh.qlen = h.m;
+      hh.tlen = T->len[ti];
+      hh.score = r.bits;
+      hh.bias = r.bias;
+      hh.evalue = evalue;
+      hh.nexpected = r.nexpected;
+      hh.ndomains = (int32_t)r.domains.size();
+      hh.domain_offset = (int32_t)out->doms.size();
+      for (const DomainOut& d : r.domains) {
+        sx_domain dd{};
+        dd.score = d.bits;
+        dd.bias = d.bias;
+        dd.c_evalue = NAN;
+        dd.i_evalue = std::exp(d.lnp) * z;
+        dd.hmm_from = (int32_t)d.kali; dd.hmm_to = (int32_t)d.mali;
+        dd.ali_from = (int32_t)d.iali; dd.ali_to = (int32_t)d.jali;
+        dd.env_from = (int32_t)d.ienv; dd.env_to = (int32_t)d.jenv;
+        dd.reported = 0;
+        out->doms.push_back(dd);
+      }
+      out->hits.push_back(hh);
+    }
+    const double dom_z = (double)std::max<size_t>(out->hits.size() - first_hit, 1);
+    for (size_t q = first_hit; q < out->hits.size(); q++) {
+      const sx_hit& hh = out->hits[q];
+      for (int d = 0; d < hh.ndomains; d++) {
+        sx_domain& dd = out->doms[hh.domain_offset + d];
+        const double p_dom = dd.i_evalue / z;
+        dd.c_evalue = p_dom * dom_z;
+        dd.reported = is_e ? (dd.c_evalue <= e_dom) : (dd.score >= t_dom);
+      }
+    }
+  }
+  return SX_OK;
+}
+
+int check_cutoffs(const sx_profiles* P, int kind) {
+  for (const ProfileHost& h : P->h) {
+    if (kind == SX_CUT_GA && !h.has_ga) return fail(SX_ECUTOFF, "GA bit thresholds unavailable on model " + h.name);
+    if (kind == SX_CUT_NC && !h.has_nc) return fail(SX_ECUTOFF, "NC bit thresholds unavailable on model " + h.name);
+    if (kind == SX_CUT_TC && !h.has_tc) return fail(SX_ECUTOFF, "TC bit thresholds unavailable on model " + h.name);
+  }
+  if (kind < SX_CUT_EVALUE || kind > SX_CUT_TC) return fail(SX_EINVAL, "unknown cutoff kind " + std::to_string(kind));
+  return SX_OK;
+}
+
+// MSV tiles: for every profile, slices of the length-sorted target order with
+// roughly equal residue counts.
+std::vector<std::vector<MsvTile>> make_all_pairs_tiles(const sx_engine* E, const sx_profiles* P, const sx_targets* T) {
+  std::vector<std::vector<MsvTile>> by_shape(kNumMsvShapes);
+  const int nt = (int)T->len.size();
+  if (nt == 0) return by_shape;
+  const int np = (int)P->h.size();
+  const int waves = 16;
+  int nslices = (int)std::ceil((double)waves * E->num_sms * 2 / std::max(1, np));
+  nslices = std::max(1, std::min(nslices, std::max(1, nt / 32)));
+  // slice boundaries with ~equal residues
+  std::vector<int> cut(nslices + 1, nt);
+  cut[0] = 0;
+  {
+    double acc = 0, per = T->residues / nslices;
+    int s = 1;
+    for (int q = 0; q < nt && s < nslices; q++) {
+      acc += T->len[T->order[q]];
+      if (acc >= per * s) cut[s++] = q + 1;
+    }
+  }
+  std::vector<int> pord(np);
+  std::iota(pord.begin(), pord.end(), 0);
+  std::stable_sort(pord.begin(), pord.end(), [&](int a, int b) { return P->h[a].m > P->h[b].m; });
+  for (int pi : pord)
+    for (int s = 0; s < nslices; s++)
+      if (cut[s + 1] > cut[s]) by_shape[P->msv_shape[pi]].push_back({pi, cut[s], cut[s + 1], 0});
+  return by_shape;
+}
+
+void launch_msv(sx_engine* E, const sx_profiles* P, const sx_targets* T, const std::vector<std::vector<MsvTile>>& tiles,
+                const int32_t* d_list, float* d_scores, const int32_t* d_slot, PairRec* surv, const BinRegion* bins,
+                unsigned* counts) {
+  const auto& K = kernels();
+  std::vector<MsvTile> all;
+  std::vector<size_t> start(kNumMsvShapes + 1, 0);
+  for (int s = 0; s < kNumMsvShapes; s++) {
+    start[s] = all.size();
+    all.insert(all.end(), tiles[s].begin(), tiles[s].end());
+  }
+  start[kNumMsvShapes] = all.size();
+  if (all.empty()) return;
+  E->tiles.upload(all.data(), all.size(), E->stream);
+  for (int s = 0; s < kNumMsvShapes; s++) {
+    const size_t nt = start[s + 1] - start[s];
+    if (!nt) continue;
+    const int g = kMsvShapes[s].g, c = kMsvShapes[s].c;
+    const size_t smem = 25ull * (c / 4) * g * sizeof(float4);
+    CK(cudaFuncSetAttribute((const void*)K.msv[s], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    K.msv[s]<<<(unsigned)nt, 256, smem, E->stream>>>(E->tiles.p + start[s], P->d_prof.p, E->thr.p, P->d_msv.p,
+                                                     T->d_res.p, T->d_off.p, T->d_len.p, T->d_tpar.p, d_list,
+                                                     d_scores, d_slot, surv, bins, counts, E->overflow.p);
+    E->stats.kernel_launches++;
+  }
+  CK(cudaGetLastError());
+}
+
+// One filter stage over per-vbin lists: stage `si` reads lists[si] and writes lists[si+1].
+void launch_stage(sx_engine* E, const sx_profiles* P, const sx_targets* T, int si, const std::vector<unsigned>& nin) {
+  const auto& K = kernels();
+  cudaStream_t s = E->stream;
+  unsigned* cin = E->counts.p + si * kNumVbins;
+  unsigned* cout = E->counts.p + (si + 1) * kNumVbins;
+  if (si == 0) {
+    unsigned mx = 0;
+    for (int b = 0; b < kNumVbins; b++) mx = std::max(mx, nin[b]);
+    if (!mx) return;
+    dim3 grid((unsigned)std::min<int64_t>((mx + 255) / 256, (int64_t)E->num_sms * 8), kNumVbins);
+    sxk::bias_kernel<<<grid, 256, 0, s>>>(E->lists[0].p, cin, E->bins[0].p, E->lists[1].p, E->bins[1].p, cout,
+                                          E->overflow.p, P->d_bias.p, E->thr.p, T->d_res.p, T->d_off.p, T->d_len.p,
+                                          kSlackBits, nullptr);
+    E->stats.kernel_launches++;
+  } else {
+    for (int b = 0; b < kNumVbins; b++) {
+      if (!nin[b]) continue;
+      const int blocks = (int)std::min<int64_t>((nin[b] + 7) / 8, (int64_t)E->num_sms * 16);
+      if (si == 1)
+        K.vit[b]<<<blocks, 256, 0, s>>>(E->lists[1].p, cin, E->bins[1].p, b, E->lists[2].p, E->bins[2].p, cout,
+                                        E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
+                                        T->d_len.p, T->d_xsc.p, kSlackBits, nullptr);
+      else
+        K.fwd[b]<<<blocks, 256, 0, s>>>(E->lists[2].p, cin, E->bins[2].p, b, E->lists[3].p, E->bins[3].p, cout,
+                                        E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
+                                        T->d_len.p, T->d_xsc.p, kSlackBits, nullptr, nullptr);
+      E->stats.kernel_launches++;
+    }
+  }
+  CK(cudaGetLastError());
+}
+
+double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx_search_cfg* cfg, sx_hits* out) {
+  int rc = check_cutoffs(P, cfg->cutoff_kind);
+  if (rc) return rc;
+  E->stats = sx_search_stats{};
+  SearchOpts o;
+  o.filters = cfg->filters != 0;
+  o.null2 = cfg->null2 != 0;
+  o.f1 = cfg->f1;
+  o.f2 = cfg->f2;
+  o.f3 = cfg->f3;
+  const size_t np = P->h.size(), nt = T->len.size();
+  cudaStream_t s = E->stream;
+  std::vector<Thresholds> th = make_thresholds(P->h, o);
+  E->thr.upload(th.data(), th.size(), s);
+  E->overflow.alloc(1);
+  E->counts.alloc(4 * kNumVbins);
+  std::vector<FinalPair> finals;
+  auto t_start = std::chrono::steady_clock::now();
+
+  // Profiles searched with filters vs. without (uncalibrated or --max): the
+  // latter send every target straight to Forward/Backward.
+  std::vector<int> unfiltered;
+  for (size_t pi = 0; pi < np; pi++)
+    if (!th[pi].exact) unfiltered.push_back((int)pi);
+  const bool any_filtered = unfiltered.size() < np;
+
+  if (any_filtered && nt > 0) {
+    // capacity per vbin from the number of pairs it holds
+    std::vector<double> pairs_in_bin(kNumVbins, 0.0);
+    double cells_total = 0;
+    for (size_t pi = 0; pi < np; pi++)
+      if (th[pi].exact) {
+        pairs_in_bin[P->dp[pi].vbin] += (double)nt;
+        cells_total += (double)P->h[pi].m * T->residues;
+      }
+    double scale = 1.0;
+    for (int attempt = 0; attempt < 4; attempt++) {
+      std::vector<double> w1(kNumVbins), w3(kNumVbins);
+      for (int b = 0; b < kNumVbins; b++) {
+        w1[b] = pairs_in_bin[b] > 0 ? std::min(pairs_in_bin[b], scale * (0.06 * pairs_in_bin[b] + 8192)) : 0;
+        w3[b] = pairs_in_bin[b] > 0 ? std::min(pairs_in_bin[b], scale * (0.01 * pairs_in_bin[b] + 4096)) : 0;
+      }
+      StageLists L0 = make_regions(w1), L1 = make_regions(w1), L2 = make_regions(w3), L3 = make_regions(w3);
+      StageLists* Ls[4] = {&L0, &L1, &L2, &L3};
+      for (int q = 0; q < 4; q++) {
+        E->lists[q].alloc((size_t)Ls[q]->total);
+        E->bins[q].upload(Ls[q]->reg.data(), kNumVbins, s);
+      }
+      CK(cudaMemsetAsync(E->counts.p, 0, sizeof(unsigned) * 4 * kNumVbins, s));
+      CK(cudaMemsetAsync(E->overflow.p, 0, sizeof(unsigned), s));
+      // stage 0: MSV over all pairs of filtered profiles
+      auto tiles = make_all_pairs_tiles(E, P, T);
+      for (auto& v : tiles)
+        v.erase(std::remove_if(v.begin(), v.end(), [&](const MsvTile& t) { return !th[t.p].exact; }), v.end());
+      CK(cudaEventRecord(E->ev[0], s));
+      launch_msv(E, P, T, tiles, T->d_order.p, nullptr, nullptr, E->lists[0].p, E->bins[0].p, E->counts.p);
+      CK(cudaEventRecord(E->ev[1], s));
+      std::vector<unsigned> cnt(4 * kNumVbins);
+      for (int si = 0; si < 3; si++) {
+        CK(cudaMemcpyAsync(cnt.data(), E->counts.p, sizeof(unsigned) * 4 * kNumVbins, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        std::vector<unsigned> nin(kNumVbins);
+        for (int b = 0; b < kNumVbins; b++) nin[b] = std::min(cnt[si * kNumVbins + b], Ls[si]->reg[b].cap);
+        CK(cudaEventRecord(E->ev[2 + si], s));
+        launch_stage(E, P, T, si, nin);
+      }
+      CK(cudaEventRecord(E->ev[5], s));
+      unsigned ovf = 0;
+      CK(cudaMemcpyAsync(cnt.data(), E->counts.p, sizeof(unsigned) * 4 * kNumVbins, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(&ovf, E->overflow.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      if (ovf) {  // a survivor list was too small: grow and rerun
+        scale *= 4.0;
+        continue;
+      }
+      // stats
+      double pairs_all = 0;
+      for (int b = 0; b < kNumVbins; b++) pairs_all += pairs_in_bin[b];
+      E->stats.pairs_in[0] = (int64_t)pairs_all;
+      E->stats.cells[0] = cells_total;
+      for (int si = 0; si < 4; si++) {
+        int64_t c = 0;
+        for (int b = 0; b < kNumVbins; b++) c += cnt[si * kNumVbins + b];
+        E->stats.pairs_out[si] = c;
+        if (si < 3) E->stats.pairs_in[si + 1] = c;
+      }
+      E->stats.ms[0] = elapsed_ms(E->ev[0], E->ev[1]);
+      E->stats.ms[1] = elapsed_ms(E->ev[2], E->ev[3]);
+      E->stats.ms[2] = elapsed_ms(E->ev[3], E->ev[4]);
+      E->stats.ms[3] = elapsed_ms(E->ev[4], E->ev[5]);
+      // gather stage-3 survivors
+      std::vector<PairRec> surv;
+      for (int b = 0; b < kNumVbins; b++) {
+        const unsigned n = std::min(cnt[3 * kNumVbins + b], L3.reg[b].cap);
+        if (!n) continue;
+        const size_t o0 = surv.size();
+        surv.resize(o0 + n);
+        CK(cudaMemcpyAsync(surv.data() + o0, E->lists[3].p + L3.reg[b].off, sizeof(PairRec) * n,
+                           cudaMemcpyDeviceToHost, s));
+      }
+      CK(cudaStreamSynchronize(s));
+      // exact host re-check of F1 / bias / F2 with the reference's libm
+      std::vector<char> keep(surv.size(), 0);
+      parallel_for(surv.size(), E->host_threads, [&](size_t i) {
+        PairRec& r = surv[i];
+        const ProfileHost& h = P->h[r.p];
+        const uint8_t* d = T->dsq.data() + T->off[r.t];
+        const int64_t l = T->len[r.t];
+        const float nullsc = null1_score(l);
+        if (gumbel_survival((double)((r.usc - nullsc) / kLn2f), h.msv[0], h.msv[1]) > o.f1) return;
+        const float fsc = composition_bias_score(h, d, l);
+        r.filtersc = fsc;
+        if (gumbel_survival((double)((r.usc - fsc) / kLn2f), h.msv[0], h.msv[1]) > o.f1) return;
+        if (gumbel_survival((double)((r.vsc - fsc) / kLn2f), h.vit[0], h.vit[1]) > o.f2) return;
+        keep[i] = 1;
+      });
+      for (size_t i = 0; i < surv.size(); i++)
+        if (keep[i]) finals.push_back({surv[i].p, surv[i].t, surv[i].usc, surv[i].filtersc, surv[i].vsc, -1});
+      break;
+    }
+  }
+  for (int pi : unfiltered)
+    for (size_t t = 0; t < nt; t++) finals.push_back({pi, (int32_t)t, 0.f, 0.f, 0.f, -1});
+  E->stats.pairs_in[4] = (int64_t)finals.size();
+
+  // Forward/Backward rows + host domain definition
+  std::vector<PairResult> res(finals.size());
+  std::atomic<int64_t> n_domain{0};
+  auto t_rows = std::chrono::steady_clock::now();
+  rows_pass(E, P, T, finals, [&](size_t i, const float* fr, const float* br) {
+    const FinalPair& f = finals[i];
+    const ProfileHost& h = P->h[f.p];
+    const int64_t l = T->len[f.t];
+    const float fwdsc = forward_score_from_rows(h, l, fr);
+    if (th[f.p].exact) {  // F3 (pipeline.rs:179-183)
+      if (std::exp(exp_tail_logsurv((double)((fwdsc - f.filtersc) / kLn2f), h.fwd[0], h.fwd[1])) > o.f3) return;
+    }
+    n_domain++;
+    RawRows rr{fr, br};
+    res[i].hit = define_domains(h, T->dsq.data() + T->off[f.t], l, rr, fwdsc, o, res[i].h);
+  });
+  auto t_end = std::chrono::steady_clock::now();
+  E->stats.pairs_out[4] = n_domain.load();
+  E->stats.ms[4] = std::chrono::duration<double, std::milli>(t_end - t_rows).count();
+  for (const auto& f : finals) E->stats.cells[4] += (double)P->h[f.p].m * T->len[f.t];
+  E->stats.ms[5] = std::chrono::duration<double, std::milli>(t_end - t_start).count();
+  std::vector<std::vector<std::pair<int32_t, HitOut>>> per(np);
+  for (size_t i = 0; i < finals.size(); i++)
+    if (res[i].hit) per[finals[i].p].emplace_back(finals[i].t, std::move(res[i].h));
+  return report(P, T, cfg, per, out);
+}
+
+}  // namespace
+
+// ================================================================ C ABI
+extern "C" {
+
+const char* sx_last_error(void) { return g_err.c_str(); }
+
+int sx_create(const sx_opts* opts, sx_engine** out) {
+  if (!out) return fail(SX_EINVAL, "sx_create: out is NULL");
+  *out = nullptr;
+  auto e = std::make_unique<sx_engine>();
+  e->device = opts ? opts->device : 0;
+  e->flags = opts ? opts->flags : 0;
+  e->host_threads = (opts && opts->host_threads > 0) ? opts->host_threads : (int)std::thread::hardware_concurrency();
+  e->host_threads = std::max(1, e->host_threads);
+  e->batch_bytes = (opts && opts->batch_bytes > 0) ? opts->batch_bytes : (2LL << 30);
+  try {
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (e->device < 0 || e->device >= ndev)
+      return fail(SX_EINVAL, "sx_create: device " + std::to_string(e->device) + " not present (" +
+                                 std::to_string(ndev) + " devices)");
+    CK(cudaSetDevice(e->device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, e->device));
+    if (prop.major < 10)
+      return fail(SX_EINVAL, std::string("sx_create: device is ") + prop.name + " (sm_" + std::to_string(prop.major) +
+                                 std::to_string(prop.minor) + "); this library is built for sm_100a");
+    e->num_sms = prop.multiProcessorCount;
+    CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    for (auto& ev : e->ev) CK(cudaEventCreate(&ev));
+    (void)kernels();
+  } catch (const CudaError& ce) {
+    return fail(ce.code, ce.msg);
+  }
+  *out = e.release();
+  return SX_OK;
+}
+
+void sx_destroy(sx_engine* e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  for (auto& ev : e->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+static int finish_profiles(sx_engine* e, std::unique_ptr<sx_profiles> p, sx_profiles** out) {
+  try {
+    CK(cudaSetDevice(e->device));
+    pack_profiles(p.get());
+  } catch (const CudaError& ce) {
+    return fail(ce.code, ce.msg);
+  }
+  *out = p.release();
+  return SX_OK;
+}
+
+int sx_profiles_load_text(sx_engine* e, const char* text, size_t len, const char* source, sx_profiles** out) {
+  if (!e || !out || (!text && len)) return fail(SX_EINVAL, "sx_profiles_load_text: NULL argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(e->mu);
+  auto p = std::make_unique<sx_profiles>();
+  p->eng = e;
+  std::string err;
+  if (!load_profiles_text(text ? text : "", len, source ? source : "<stream>", p->h, err)) return fail(SX_EINVAL, err);
+  return finish_profiles(e, std::move(p), out);
+}
+
+int sx_profiles_load_file(sx_engine* e, const char* path, sx_profiles** out) {
+  if (!e || !out || !path) return fail(SX_EINVAL, "sx_profiles_load_file: NULL argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(e->mu);
+  auto p = std::make_unique<sx_profiles>();
+  p->eng = e;
+  std::string err;
+  bool io = false;
+  if (!load_profiles_file(path, p->h, err, io)) return fail(io ? SX_EIO : SX_EINVAL, err);
+  return finish_profiles(e, std::move(p), out);
+}
+
+int32_t sx_profiles_count(const sx_profiles* p) { return p ? (int32_t)p->h.size() : 0; }
+
+int sx_profiles_info(const sx_profiles* p, int32_t i, sx_profile_info* out) {
+  if (!p || !out || i < 0 || i >= (int32_t)p->h.size()) return fail(SX_EINVAL, "sx_profiles_info: bad index");
+  const ProfileHost& h = p->h[i];
+  out->name = h.name.c_str();
+  out->acc = h.has_acc ? h.acc.c_str() : nullptr;
+  out->desc = h.has_desc ? h.desc.c_str() : nullptr;
+  out->m = h.m;
+  out->calibrated = h.calibrated();
+  for (int q = 0; q < 2; q++) {
+    out->ga[q] = h.has_ga ? h.ga[q] : NAN;
+    out->tc[q] = h.has_tc ? h.tc[q] : NAN;
+    out->nc[q] = h.has_nc ? h.nc[q] : NAN;
+    out->msv[q] = h.has_msv ? h.msv[q] : NAN;
+    out->viterbi[q] = h.has_vit ? h.vit[q] : NAN;
+    out->forward[q] = h.has_fwd ? h.fwd[q] : NAN;
+  }
+  return SX_OK;
+}
+
+void sx_profiles_free(sx_profiles* p) {
+  if (!p) return;
+  cudaSetDevice(p->eng->device);
+  delete p;
+}
+
+static int finish_targets(sx_engine* e, std::unique_ptr<sx_targets> t, sx_targets** out) {
+  t->dsq.resize(t->dsq.size() + 64, SYM_STAR);  // read slack past the last target
+  try {
+    CK(cudaSetDevice(e->device));
+    pack_targets(t.get());
+  } catch (const CudaError& ce) {
+    return fail(ce.code, ce.msg);
+  }
+  *out = t.release();
+  return SX_OK;
+}
+
+int sx_targets_create(sx_engine* e, const char* const* ids, const uint8_t* const* seqs, const size_t* lens, size_t n,
+                      sx_targets** out) {
+  if (!e || !out || (n && (!seqs || !lens))) return fail(SX_EINVAL, "sx_targets_create: NULL argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(e->mu);
+  auto t = std::make_unique<sx_targets>();
+  t->eng = e;
+  std::vector<uint8_t> dig;
+  for (size_t i = 0; i < n; i++) {
+    dig.clear();
+    for (size_t q = 0; q < lens[i]; q++) {
+      const uint8_t b = seqs[i][q];
+      if (b == ' ' || b == '\t' || b == '\n' || b == '\r' || b == '\f' || b == '\v') continue;
+      dig.push_back(kDigitize[b]);
+    }
+    if (dig.size() > (size_t)INT32_MAX) return fail(SX_EINVAL, "sx_targets_create: sequence too long");
+    append_target(t.get(), dig.data(), dig.size());
+    t->ids.push_back(ids && ids[i] ? ids[i] : std::to_string(i));
+  }
+  return finish_targets(e, std::move(t), out);
+}
+
+int sx_targets_create_digital(sx_engine* e, const uint8_t* dsq, const int64_t* offsets, const int64_t* lens, size_t n,
+                              sx_targets** out) {
+  if (!e || !out || (n && (!dsq || !offsets || !lens))) return fail(SX_EINVAL, "sx_targets_create_digital: NULL argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(e->mu);
+  auto t = std::make_unique<sx_targets>();
+  t->eng = e;
+  for (size_t i = 0; i < n; i++) {
+    if (lens[i] < 0 || offsets[i] < 0 || lens[i] > INT32_MAX) return fail(SX_EINVAL, "sx_targets_create_digital: bad length");
+    for (int64_t q = 0; q < lens[i]; q++)
+      if (dsq[offsets[i] + q] > SYM_STAR)
+        return fail(SX_EINVAL, "sx_targets_create_digital: residue code " + std::to_string(dsq[offsets[i] + q]) +
+                                   " out of range in target " + std::to_string(i));
+    append_target(t.get(), dsq + offsets[i], (size_t)lens[i]);
+    t->ids.push_back(std::to_string(i));
+  }
+  return finish_targets(e, std::move(t), out);
+}
+
+int64_t sx_targets_count(const sx_targets* t) { return t ? (int64_t)t->len.size() : 0; }
+
+void sx_targets_free(sx_targets* t) {
+  if (!t) return;
+  cudaSetDevice(t->eng->device);
+  delete t;
+}
+
+int sx_search(sx_engine* e, const sx_profiles* p, const sx_targets* t, const sx_search_cfg* cfg, sx_hits** out) {
+  if (!e || !p || !t || !cfg || !out) return fail(SX_EINVAL, "sx_search: NULL argument");
+  if (p->eng != e || t->eng != e) return fail(SX_EINVAL, "sx_search: profiles/targets belong to another engine");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(e->mu);
+  auto h = std::make_unique<sx_hits>();
+  try {
+    CK(cudaSetDevice(e->device));
+    const int rc = run_search(e, p, t, cfg, h.get());
+    if (rc) return rc;
+  } catch (const CudaError& ce) {
+    return fail(ce.code, ce.msg);
+  } catch (const std::bad_alloc&) {
+    return fail(SX_ENOMEM, "sx_search: host allocation failed");
+  }
+  *out = h.release();
+  return SX_OK;
+}
+
+size_t sx_hits_count(const sx_hits* h) { return h ? h->hits.size() : 0; }
+const sx_hit* sx_hits_array(const sx_hits* h) { return h && !h->hits.empty() ? h->hits.data() : nullptr; }
+size_t sx_hits_domain_count(const sx_hits* h) { return h ? h->doms.size() : 0; }
+const sx_domain* sx_hits_domains(const sx_hits* h) { return h && !h->doms.empty() ? h->doms.data() : nullptr; }
+void sx_hits_free(sx_hits* h) { delete h; }
+
+int sx_last_search_stats(const sx_engine* e, sx_search_stats* out) {
+  if (!e || !out) return fail(SX_EINVAL, "sx_last_search_stats: NULL argument");
+  *out = e->stats;
+  return SX_OK;
+}
+
+int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, const int32_t* pair_profile,
+                   const int32_t* pair_target, size_t npairs, float* msv, float* viterbi, float* forward,
+                   float* backward, float* bias) {
+  if (!e || !p || !t || (npairs && (!pair_profile || !pair_target))) return fail(SX_EINVAL, "sx_score_pairs: NULL argument");
+  std::lock_guard<std::mutex> lk(e->mu);
+  const size_t np = p->h.size(), nt = t->len.size();
+  for (size_t i = 0; i < npairs; i++)
+    if (pair_profile[i] < 0 || (size_t)pair_profile[i] >= np || pair_target[i] < 0 || (size_t)pair_target[i] >= nt)
+      return fail(SX_EINVAL, "sx_score_pairs: pair " + std::to_string(i) + " out of range");
+  if (!npairs) return SX_OK;
+  try {
+    CK(cudaSetDevice(e->device));
+    cudaStream_t s = e->stream;
+    e->stats = sx_search_stats{};
+    std::vector<Thresholds> th(np, Thresholds{-INFINITY, -INFINITY, -INFINITY, 0});
+    e->thr.upload(th.data(), th.size(), s);
+    e->overflow.alloc(1);
+    CK(cudaMemsetAsync(e->overflow.p, 0, sizeof(unsigned), s));
+    e->scores.alloc(npairs);
+    if (msv) {
+      // list sorted by (profile, length desc); tiles per profile over that list
+      std::vector<int32_t> idx(npairs);
+      std::iota(idx.begin(), idx.end(), 0);
+      std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+        if (pair_profile[a] != pair_profile[b]) return pair_profile[a] < pair_profile[b];
+        return t->len[pair_target[a]] > t->len[pair_target[b]];
+      });
+      std::vector<int32_t> lst(npairs), slot(npairs);
+      for (size_t q = 0; q < npairs; q++) {
+        lst[q] = pair_target[idx[q]];
+        slot[q] = idx[q];
+      }
+      std::vector<std::vector<MsvTile>> tiles(kNumMsvShapes);
+      size_t q = 0;
+      while (q < npairs) {
+        size_t r = q;
+        const int pp = pair_profile[idx[q]];
+        while (r < npairs && pair_profile[idx[r]] == pp) r++;
+        for (size_t a = q; a < r; a += 4096)
+          tiles[p->msv_shape[pp]].push_back({pp, (int32_t)a, (int32_t)std::min(r, a + 4096), 0});
+        q = r;
+      }
+      e->plist.upload(lst.data(), npairs, s);
+      e->slots.upload(slot.data(), npairs, s);
+      launch_msv(e, p, t, tiles, e->plist.p, e->scores.p, e->slots.p, nullptr, nullptr, nullptr);
+      CK(cudaMemcpyAsync(msv, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+    }
+    if (bias || viterbi) {
+      // pair lists per vbin, every pair carries its slot
+      std::vector<PairRec> recs;
+      std::vector<BinRegion> reg(kNumVbins);
+      std::vector<unsigned> cnt(kNumVbins, 0);
+      std::vector<std::vector<int32_t>> byb(kNumVbins);
+      for (size_t i = 0; i < npairs; i++) byb[p->dp[pair_profile[i]].vbin].push_back((int32_t)i);
+      for (int b = 0; b < kNumVbins; b++) {
+        reg[b].off = (int64_t)recs.size();
+        reg[b].cap = (uint32_t)byb[b].size();
+        reg[b].pad = 0;
+        cnt[b] = (unsigned)byb[b].size();
+        for (int32_t i : byb[b]) recs.push_back({pair_profile[i], pair_target[i], 0.f, 0.f, 0.f, 0.f, i, 0});
+      }
+      e->lists[0].upload(recs.data(), recs.size(), s);
+      e->bins[0].upload(reg.data(), reg.size(), s);
+      e->counts.alloc(4 * kNumVbins);
+      CK(cudaMemcpyAsync(e->counts.p, cnt.data(), sizeof(unsigned) * kNumVbins, cudaMemcpyHostToDevice, s));
+      const auto& K = kernels();
+      if (bias) {
+        unsigned mx = *std::max_element(cnt.begin(), cnt.end());
+        dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>((mx + 255) / 256, (int64_t)e->num_sms * 8)), kNumVbins);
+        sxk::bias_kernel<<<grid, 256, 0, s>>>(e->lists[0].p, e->counts.p, e->bins[0].p, nullptr, nullptr, nullptr,
+                                              e->overflow.p, p->d_bias.p, e->thr.p, t->d_res.p, t->d_off.p, t->d_len.p,
+                                              0.f, e->scores.p);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(bias, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+      }
+      if (viterbi) {
+        for (int b = 0; b < kNumVbins; b++) {
+          if (!cnt[b]) continue;
+          const int blocks = (int)std::min<int64_t>((cnt[b] + 7) / 8, (int64_t)e->num_sms * 16);
+          K.vit[b]<<<blocks, 256, 0, s>>>(e->lists[0].p, e->counts.p, e->bins[0].p, b, nullptr, nullptr, nullptr,
+                                          e->overflow.p, p->d_prof.p, e->thr.p, p->d_vfb.p, t->d_res.p, t->d_off.p,
+                                          t->d_len.p, t->d_xsc.p, 0.f, e->scores.p);
+        }
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(viterbi, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+      }
+    }
+    if (forward || backward) {
+      std::vector<FinalPair> fp(npairs);
+      for (size_t i = 0; i < npairs; i++) fp[i] = {pair_profile[i], pair_target[i], 0.f, 0.f, 0.f, (int32_t)i};
+      rows_pass(e, p, t, fp, [&](size_t i, const float* fr, const float* br) {
+        const ProfileHost& h = p->h[fp[i].p];
+        const int64_t l = t->len[fp[i].t];
+        if (l == 0 || h.m == 0) {
+          if (forward) forward[i] = kNegInf;
+          if (backward) backward[i] = kNegInf;
+          return;
+        }
+        if (forward) forward[i] = forward_score_from_rows(h, l, fr);
+        if (backward) backward[i] = backward_score_from_rows(l, br);
+      });
+    }
+  } catch (const CudaError& ce) {
+    return fail(ce.code, ce.msg);
+  }
+  return SX_OK;
+}
+
+int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, const int32_t* pair_profile,
+                      const int32_t* pair_target, size_t npairs, int32_t m, float* d_msc, float* d_isc,
+                      float* d_trans, double* lnz) {
+  (void)e; (void)p; (void)t; (void)pair_profile; (void)pair_target; (void)npairs; (void)m;
+  (void)d_msc; (void)d_isc; (void)d_trans; (void)lnz;
+  return fail(SX_EINVAL, "sx_posterior_grad: not available in this build");
+}
+
+}  // extern "C"

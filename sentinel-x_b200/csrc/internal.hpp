@@ -1,0 +1,114 @@
+// Internal host-side types of the sxhmm engine.
+#pragma once
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <limits>
+#include <string>
+#include <vector>
+
+namespace sx {
+
+constexpr int NRES = 20;   // canonical residues, HMMER order ACDEFGHIKLMNPQRSTVWY
+constexpr int NSYM = 25;   // + B J Z X and the nonresidue '*'
+constexpr uint8_t SYM_STAR = 24;
+constexpr float kNegInf = -std::numeric_limits<float>::infinity();
+constexpr float kLn2f = 0.693147182464599609375f;  // f32 rounding of ln 2
+
+// HMMER3's amino-acid background (p7_AminoFrequencies), src/hmmer/alphabet.rs:36-39.
+extern const float kBackground[NRES];
+// Members of the degenerate codes B, J, Z, X (src/hmmer/alphabet.rs:42-54).
+struct Degenerate {
+  int n;
+  int members[20];
+};
+const Degenerate& degenerate(int code);  // code in 20..23
+// ASCII -> digital code (src/hmmer/alphabet.rs:58-88): case-insensitive, U->C,
+// O->K, gap/stop characters -> '*', other letters -> X, everything else -> '*'.
+extern const uint8_t kDigitize[256];
+
+// Transition slots of a node, in HMMER file order.
+enum Tr { TMM = 0, TMI, TMD, TIM, TII, TDM, TDD, TBM, NTR };
+
+// One configured profile (HMMER p7_ProfileConfig, local multihit;
+// src/hmmer/model.rs:146-245).  Vectors have M+1 entries indexed by node k.
+struct ProfileHost {
+  std::string name, acc, desc;
+  bool has_acc = false, has_desc = false;
+  int m = 0;
+  bool has_ga = false, has_tc = false, has_nc = false;
+  float ga[2] = {NAN, NAN}, tc[2] = {NAN, NAN}, nc[2] = {NAN, NAN};
+  bool has_msv = false, has_vit = false, has_fwd = false;
+  double msv[2] = {NAN, NAN}, vit[2] = {NAN, NAN}, fwd[2] = {NAN, NAN};
+  bool calibrated() const { return has_msv && has_vit && has_fwd; }
+  std::vector<float> msc;  // [NSYM][M+1] log-odds match scores (nats)
+  std::vector<float> mo;   // [NSYM][M+1] match odds exp(msc)
+  std::vector<float> t[NTR];  // log-space transitions, node k (t[TBM] = local entry B->M_k)
+  std::vector<float> p[NTR];  // probability-space copies
+  float msv_tbm = 0;
+  float compo[NRES];
+  const float* msc_row(int x) const { return msc.data() + (size_t)x * (m + 1); }
+  const float* mo_row(int x) const { return mo.data() + (size_t)x * (m + 1); }
+};
+
+// Parse (plain or gzip) HMMER3 text and configure every profile.  Returns
+// false with `err` set (messages follow src/hmmer/parse.rs: "<source> line N: ...").
+bool load_profiles_text(const char* text, size_t len, const std::string& source, std::vector<ProfileHost>& out,
+                        std::string& err);
+bool load_profiles_file(const std::string& path, std::vector<ProfileHost>& out, std::string& err, bool& io_error);
+
+// Length-dependent special transitions (p7_ReconfigLength; src/hmmer/model.rs:284-312).
+struct SpecialTr {
+  float loop, move;    // N/J/C loop and move, log space
+  float e_move, e_loop;
+  float ploop, pmove;  // probability space
+  float pe_move, pe_loop;
+};
+SpecialTr special_transitions(int64_t l, bool multihit);
+float null1_score(int64_t l);  // src/hmmer/model.rs:334-337
+
+// ---- host-side domain definition (the per-hit tail of score_target) ----
+struct SearchOpts {
+  bool filters = true, null2 = true;
+  double f1 = 0.02, f2 = 1e-3, f3 = 1e-5;
+};
+
+struct DomainOut {
+  int64_t ienv, jenv, iali, jali, kali, mali;
+  float bits, bias;
+  double lnp;
+};
+struct HitOut {
+  float bits, bias;
+  double lnp;
+  float nexpected;
+  int64_t nregions;
+  std::vector<DomainOut> domains;
+};
+
+// Raw, still-scaled Forward / Backward special-state rows produced on the
+// device: per row i the five values N B E J C and the row's rescale factor
+// (0 when the row was not rescaled).
+struct RawRows {
+  const float* fwd;  // (L+1) x 6, row 0 unused
+  const float* bwd;  // (L+1) x 6; row 0 holds the B sum in slot 1
+};
+
+// From the raw rows: exact Forward/Backward scores and special rows (using
+// the same libm as the reference), then posterior decoding, region
+// identification, envelope rescoring, null2 and final scores
+// (src/hmmer/pipeline.rs:187-293).  Returns false when the pair yields no hit.
+// `fwdsc_out` receives the Forward score (for the F3 decision by the caller).
+float forward_score_from_rows(const ProfileHost& p, int64_t l, const float* fwd_rows);
+float backward_score_from_rows(int64_t l, const float* bwd_rows);
+bool define_domains(const ProfileHost& p, const uint8_t* dsq, int64_t l, const RawRows& rows, float fwdsc,
+                    const SearchOpts& o, HitOut& out);
+
+// bias_filter_score (src/hmmer/pipeline.rs:107-150), exact host version.
+float composition_bias_score(const ProfileHost& p, const uint8_t* dsq, int64_t l);
+
+// P-values (src/hmmer/pipeline.rs:87-104).
+double gumbel_survival(double x, double mu, double lambda);
+double exp_tail_logsurv(double x, double tau, double lambda);
+
+}  // namespace sx

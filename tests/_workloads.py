@@ -1,0 +1,69 @@
+"""Shared inputs for the tests: the reference fixtures, edge-case targets and
+small seeded synthetic workloads calibrated with the oracle."""
+import functools
+import os
+
+import numpy as np
+
+from oracle import oracle as O
+from sxhmm import synth
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def fixture_text():
+    return open(os.path.join(GOLDEN, "hmmer34_pair.hmm")).read()
+
+
+def tiny_text():
+    return open(os.path.join(GOLDEN, "tiny.hmm")).read()
+
+
+def fixture_targets():
+    return O.read_fasta(os.path.join(GOLDEN, "hmmer34_targets.faa"))
+
+
+def oracle_scorer(profiles, seqs):
+    """Calibration scorer backed by the oracle (tests only)."""
+    text = "".join(synth.profile_text(p) for p in profiles)
+    o = O.Oracle(text=text)
+    msv = np.zeros((len(profiles), len(seqs)))
+    vit = np.zeros_like(msv)
+    fwd = np.zeros_like(msv)
+    for i in range(len(profiles)):
+        for j, s in enumerate(seqs):
+            msv[i, j] = o.msv(i, s)
+            vit[i, j] = o.viterbi(i, s)
+            fwd[i, j] = o.forward(i, s)
+    return msv, vit, fwd
+
+
+@functools.lru_cache(maxsize=None)
+def small_config(idx, scale):
+    """A shrunk benchmark config, calibrated with the oracle."""
+    return synth.make_config(idx, scale=scale, scorer=oracle_scorer)
+
+
+def edge_targets():
+    """Targets that exercise the edges the reference handles: a single
+    residue, degenerate codes, stop/gap characters, lower case, U/O, runs of
+    '*', one long sequence."""
+    rng = np.random.default_rng(5)
+    long = "".join(synth.AA[x] for x in synth.background_seq(rng, 2500))
+    return [
+        ("one", "M"),
+        ("two", "MK"),
+        ("degen", "BJZXBJZXMKABJZX"),
+        ("stops", "MKA*MKA-MKA.MKA"),
+        ("allstop", "****"),
+        ("lower_uo", "gggmkaggguuooxxmka"),
+        ("motif", "GGGGMKAGGGG"),
+        ("two_copies", "GGGGGMKAGGGGGGGGGGGGGGGGGGGGMKAGGGGG"),
+        ("long", long),
+    ]
+
+
+def small_profiles_text(seed=3, ms=(1, 2, 5, 33, 64, 65, 129, 300)):
+    """Uncalibrated synthetic profiles of awkward lengths (lane/chunk edges)."""
+    rng = np.random.default_rng(seed)
+    return "".join(synth.profile_text(synth.sample_profile(rng, m, f"edge{m}")) for m in ms)

@@ -1,0 +1,191 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+* stage scores (msv, viterbi, forward, backward): bit-identical to the oracle
+  (which is pinned to the reference's fixtures); bias-filter score within 2 f32
+  ulps (the device evaluates it with the device log for filtering only; the
+  host recomputes it exactly before any decision is final);
+* full searches: identical hit and domain sets, bit-identical scores and
+  identical coordinates, on the HMMER 3.4 fixture (filters off), the unit-test
+  known answers, edge-case targets and seeded synthetic workloads with filters
+  on (so MSV/bias/Viterbi/Forward decisions are compared too).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+import sxhmm
+from _workloads import (edge_targets, fixture_targets, fixture_text, small_config, small_profiles_text,
+                        tiny_text)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def engine():
+    e = sxhmm.Engine()
+    yield e
+    e.close()
+
+
+def _same(a, b):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    return np.array_equal(a, b) or bool(np.all((a == b) | (np.isnan(a) & np.isnan(b))))
+
+
+def _ulps(a, b):
+    a = np.asarray(a, np.float32).view(np.int32).astype(np.int64)
+    b = np.asarray(b, np.float32).view(np.int32).astype(np.int64)
+    return np.abs(a - b)
+
+
+def _stage_check(engine, text, seqs):
+    o = O.Oracle(text=text)
+    ps = engine.load_text(text)
+    ts = engine.targets([s for _, s in seqs])
+    dsq = [O.encode(s) for _, s in seqs]
+    pp, pt = np.meshgrid(np.arange(o.n), np.arange(len(seqs)), indexing="ij")
+    pp, pt = pp.ravel(), pt.ravel()
+    got = engine.score_pairs(ps, ts, pp, pt)
+    want = {k: np.zeros(len(pp), np.float32) for k in got}
+    for q, (i, j) in enumerate(zip(pp, pt)):
+        d = dsq[j]
+        if len(d) == 0:
+            continue
+        want["msv"][q] = o.msv(i, d)
+        want["viterbi"][q] = o.viterbi(i, d)
+        want["forward"][q] = o.forward(i, d)
+        want["backward"][q] = o.backward(i, d)
+        want["bias"][q] = o.bias(i, d)
+    for k in ("msv", "viterbi", "forward", "backward"):
+        bad = np.nonzero(~((got[k] == want[k]) | (np.isnan(got[k]) & np.isnan(want[k]))))[0]
+        assert bad.size == 0, (k, [(int(pp[b]), int(pt[b]), got[k][b], want[k][b]) for b in bad[:5]])
+    assert _ulps(got["bias"], want["bias"]).max() <= 2
+    return got
+
+
+def test_stage_scores_fixture(engine):
+    _stage_check(engine, fixture_text(), fixture_targets())
+
+
+def test_stage_scores_edges(engine):
+    text = tiny_text() + small_profiles_text()
+    _stage_check(engine, text, edge_targets() + fixture_targets()[:3])
+
+
+def test_stage_scores_synthetic(engine):
+    w = small_config(1, 0.004)
+    seqs = [(f"t{i}", "".join("ACDEFGHIKLMNPQRSTVWY"[x] for x in s)) for i, s in enumerate(w.targets[:60])]
+    _stage_check(engine, w.hmm_text(), seqs)
+
+
+def _hits_oracle(text, seqs, cfg):
+    o = O.Oracle(text=text)
+    t = O.TargetBatch([O.encode(s) for _, s in seqs])
+    hits, doms = o.search(t, cfg)
+    out = []
+    for h in hits:
+        ds = [(d.score, d.bias, d.hmm_from, d.hmm_to, d.ali_from, d.ali_to, d.env_from, d.env_to, bool(d.reported),
+               d.i_evalue, d.c_evalue) for d in doms[h.dom_offset:h.dom_offset + h.ndom]]
+        out.append((h.profile_index, h.target_index, h.score, h.bias, h.evalue, h.nexpected, ds))
+    return out
+
+
+def _hits_gpu(engine, text, seqs, cfg_kw):
+    ps = engine.load_text(text)
+    targets = sxhmm.Targets(seqs)
+    cutoff = {"E": sxhmm.Cutoff.evalue(cfg_kw.get("seq", 10.0), cfg_kw.get("dom", 10.0)),
+              "T": sxhmm.Cutoff.bits(cfg_kw.get("seq", 0.0), cfg_kw.get("dom", 0.0)),
+              "GA": sxhmm.Cutoff.gathering(), "NC": sxhmm.Cutoff.noise(), "TC": sxhmm.Cutoff.trusted()}[
+        cfg_kw.get("cutoff", "E")]
+    sc = sxhmm.SearchConfig(cutoff, sxhmm.PipelineConfig(filters=cfg_kw.get("filters", True)), cfg_kw.get("z"))
+    hits = sxhmm.search_profiles(ps, targets, sc, engine)
+    out = []
+    for h in hits:
+        ds = [(d.score, d.bias, d.hmm_from, d.hmm_to, d.ali_from, d.ali_to, d.env_from, d.env_to, d.reported,
+               d.i_evalue, d.c_evalue) for d in h.domains]
+        pi = [i["name"] for i in ps.info].index(h.profile)
+        out.append((pi, h.target_index, h.score, h.bias, h.evalue, h.nexpected, ds))
+    return out
+
+
+def _assert_same_hits(a, b):
+    assert len(a) == len(b), (len(a), len(b), [x[:2] for x in a], [x[:2] for x in b])
+    for x, y in zip(a, b):
+        assert x[:2] == y[:2]
+        assert np.float32(x[2]) == np.float32(y[2]) and np.float32(x[3]) == np.float32(y[3]), (x[:4], y[:4])
+        assert (x[4] == y[4]) or (np.isnan(x[4]) and np.isnan(y[4]))
+        assert np.float32(x[5]) == np.float32(y[5])
+        assert len(x[6]) == len(y[6])
+        for d, e in zip(x[6], y[6]):
+            assert d[:9] == tuple(e[:9]) or (np.float32(d[0]) == np.float32(e[0]) and d[2:9] == tuple(e[2:9])), (d, e)
+
+
+def _cmp(engine, text, seqs, **kw):
+    ocfg = O.make_cfg(cutoff=kw.get("cutoff", "E"), seq=kw.get("seq", 10.0 if kw.get("cutoff", "E") == "E" else 0.0),
+                      dom=kw.get("dom", 10.0 if kw.get("cutoff", "E") == "E" else 0.0),
+                      filters=kw.get("filters", True), z=kw.get("z"))
+    a = _hits_oracle(text, seqs, ocfg)
+    b = _hits_gpu(engine, text, seqs, kw)
+    _assert_same_hits(a, b)
+    return a, b
+
+
+def test_search_hmmer34_fixture(engine):
+    """hmmsearch --max on the HMMER 3.4 fixture: identical to the oracle and
+    within 0.1 bits / exact coordinates of HMMER 3.4 (search.rs:316-355)."""
+    seqs = fixture_targets()
+    _, hits = _cmp(engine, fixture_text(), seqs, filters=False)
+    import os
+    from _workloads import GOLDEN
+    rows = [l.split("\t") for l in open(os.path.join(GOLDEN, "hmmer34_expected.tsv")).read().splitlines()]
+    names = [n for n, _ in seqs]
+    pnames = ["FAM14", "FAM18"]
+    for r in rows:
+        h = [x for x in hits if names[x[1]] == r[0] and pnames[x[0]] == r[1]][0]
+        assert abs(h[2] - float(r[2])) <= 0.1 and abs(h[3] - float(r[3])) <= 0.1
+        rep = [d for d in h[6] if d[8]]
+        d = rep[int(r[4]) - 1]
+        assert abs(d[0] - float(r[5])) <= 0.1
+        assert list(d[2:8]) == [int(v) for v in (r[7], r[8], r[9], r[10], r[11], r[12])]
+
+
+def test_search_fixture_filters_on(engine):
+    _cmp(engine, fixture_text(), fixture_targets(), filters=True)
+
+
+def test_search_unit_known_answers(engine):
+    a, b = _cmp(engine, tiny_text(), [("s", "GGGGGMKAGGGGGGGGGGGGGGGGGGGGMKAGGGGG")], cutoff="T", seq=-1e9, dom=-1e9,
+                filters=False)
+    assert len(b) == 1 and len(b[0][6]) == 2 and (b[0][6][0][4], b[0][6][0][5]) == (6, 8)
+    a, b = _cmp(engine, tiny_text(), [("hit", "GGGGMKAGGGG"), ("miss", "WWWWWWWWWWW")], cutoff="T", seq=0.0, dom=0.0,
+                filters=False)
+    assert len(b) == 1 and b[0][1] == 0 and b[0][6][0][8]
+
+
+def test_missing_cutoff_raises_like_reference(engine):
+    ps = engine.load_text(tiny_text())
+    with pytest.raises(sxhmm.HmmError, match="TC bit thresholds unavailable on model tiny"):
+        sxhmm.search_profiles(ps, sxhmm.Targets([("s", "MKA")]), sxhmm.SearchConfig(sxhmm.Cutoff.trusted()), engine)
+
+
+def test_search_edges(engine):
+    text = tiny_text() + small_profiles_text()
+    _cmp(engine, text, edge_targets(), cutoff="T", seq=-1e9, dom=-1e9, filters=False)
+
+
+@pytest.mark.parametrize("cutoff", ["E", "GA", "NC", "TC"])
+def test_search_synthetic_config0(engine, cutoff):
+    w = small_config(0, 0.2)
+    seqs = [(w.target_ids[i], "".join("ACDEFGHIKLMNPQRSTVWY"[x] for x in s)) for i, s in enumerate(w.targets)]
+    a, b = _cmp(engine, w.hmm_text(), seqs, cutoff=cutoff, filters=True)
+    if cutoff == "E":
+        assert len(b) >= 5  # the planted homologs are found
+
+
+def test_search_synthetic_multiprofile(engine):
+    w = small_config(1, 0.01)
+    seqs = [(w.target_ids[i], "".join("ACDEFGHIKLMNPQRSTVWY"[x] for x in s)) for i, s in enumerate(w.targets)]
+    _cmp(engine, w.hmm_text(), seqs, filters=True)
+    st = engine.stats()
+    assert st["pairs_in"][0] == len(w.profiles) * len(seqs)

@@ -1,0 +1,305 @@
+"""Benchmark: Plan7 hmmsearch GCUPS on one B200 (Pfam-scale batch).
+
+Workload (the Pfam-scale configuration): 1,000 synthetic Plan7 profiles with
+M log-normal (median 150, clipped 20..1,000) against 50,000 synthetic proteins
+with L log-normal (median 300, clipped 30..3,000), 2% carrying a planted
+homolog; STATS calibrated on the device; default hmmsearch thresholds
+(E <= 10, F1 = 0.02, F2 = 1e-3, F3 = 1e-5).  A step is one full search
+(every profile x every target through MSV -> bias -> Viterbi -> Forward,
+Backward, domain definition and reporting).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value  = sum over pairs of M*L / device time of the step (inputs resident on
+         the device, L2 flushed between steps), whole job over all ranks.
+e2e    = same metric through the public C ABI with host buffers: digitised
+         targets copied host->device, search, hits read back, every step.
+Under torchrun (N > 1) each rank searches its own block of 1,000 profiles
+against the same targets (profile-block sharding, no data-path collective).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sentinel-x_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Plan7 GCUPS (MSV/Vit/Fwd/Bwd), batched vs plain on 1 B200; hits bit-exact"
+WORKLOAD = ("pfam_scale: 1000 profiles M~LN(150,0.5)[20,1000] x 50000 targets L~LN(300,0.6)[30,3000], "
+            "2% planted homologs, E<=10, F1/F2/F3 = 0.02/1e-3/1e-5")
+MSV_OPS_PER_CELL = 3  # 1 FADD + 2 FMAX per cell (src/hmmer/dp.rs:122-124)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="sxhmm", choices=["sxhmm", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="shrink profile/target counts (testing only)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain", action="store_true", help="also time the plain one-pair-per-block kernels")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload(scale, rank, scorer=None):
+    from sxhmm import synth
+    cache = os.environ.get("SXHMM_BENCH_CACHE", "/tmp/sxhmm_bench_cache")
+    os.makedirs(cache, exist_ok=True)
+    key = os.path.join(cache, f"cfg1_s{scale}_r{rank}.npz")
+    if os.path.exists(key):
+        z = np.load(key, allow_pickle=False)
+        return str(z["text"]), z["seq"], z["offs"], z["lens"], int(z["ntarg"])
+    w = synth.make_config(1, scale=scale, seed=None if rank == 0 else 1001 + 7919 * rank, scorer=scorer)
+    if rank:
+        # every rank searches the same targets with its own profile block
+        w0 = synth.make_config(1, scale=scale)
+        w.targets = w0.targets
+    text = w.hmm_text()
+    lens = w.lens
+    offs = np.zeros(len(lens), np.int64)
+    offs[1:] = np.cumsum(lens)[:-1]
+    seq = np.concatenate(w.targets).astype(np.uint8)
+    np.savez(key, text=np.array(text), seq=seq, offs=offs, lens=lens, ntarg=len(lens))
+    return text, seq, offs, lens, len(lens)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def sha1(text):
+    import hashlib
+    return hashlib.sha1(text.encode()).hexdigest()[:16]
+
+
+def cpu_baseline(text, seq, offs, lens, seconds, as_line=False):
+    """The oracle's threaded driver (a C++ restatement of the reference's
+    rayon pair loop) on a bounded, deterministic sample of the workload: the
+    first n targets x every profile, n chosen for ~`seconds` of CPU work."""
+    from oracle import oracle as O
+    o = O.Oracle(text=text)
+    nt = len(lens)
+    cfg = O.make_cfg()
+    # sample: a strided subset of targets, all profiles (so M covers the distribution)
+    ms = np.array(o.m, dtype=np.float64)
+    stride = max(1, nt // 400)
+    pick = np.arange(0, nt, stride)[:400]
+    sub = O.TargetBatch([seq[offs[i]:offs[i] + lens[i]] for i in pick])
+    threads = os.cpu_count() or 1
+    r = o.time_pairs(sub, cfg, nthreads=threads, time_limit=seconds)
+    gcups = r["cells"] / r["seconds"] / 1e9 if r["seconds"] > 0 else None
+    return {"value": gcups, "unit": "GCUPS", "cores": threads, "kind": "port",
+            "sample": f"{r['pairs']} pairs ({r['cells']:.3e} cells) of {len(pick)} strided targets x "
+                      f"{o.n} profiles (profile-major), oracle score_target pipeline, {r['seconds']:.1f} s",
+            "pairs": r["pairs"], "seconds": r["seconds"]}
+
+
+def flush_l2(torch, buf):
+    buf.add_(1.0)  # 256 MiB write > 126 MB L2
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    text, seq, offs, lens, nt = workload(args.scale, 0, scorer=O.calibration_scorer())
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(text, seq, offs, lens, max(2.0, args.cpu_seconds / max(1, args.steps)))
+        if i >= args.warmup:
+            vals.append(r)
+    v = statistics.median([x["value"] for x in vals])
+    line = {"metric": METRIC, "value": v, "unit": "GCUPS", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": vals[-1]["sample"], "hmm_sha1": sha1(text)},
+            "cpu_baseline": {k: vals[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["cpu_baseline"]["value"] = v
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    import sxhmm
+    from sxhmm import synth
+    eng = sxhmm.Engine(device=local)
+    t0 = time.time()
+    text, seq, offs, lens, nt = workload(args.scale, rank, scorer=synth.engine_scorer(eng))
+    gen_s = time.time() - t0
+    ps = eng.load_text(text, source="pfam_scale")
+    ms = np.array([i["m"] for i in ps.info], dtype=np.float64)
+    cells = float(ms.sum()) * float(lens.sum())
+    ts = eng.targets_digital(seq, offs, lens)
+    cfg = sxhmm.SearchConfig().to_c()
+    l2 = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-resident steps ----
+    for _ in range(args.warmup):
+        eng.search(ps, ts, cfg)
+    sampler = ClockSampler(local)
+    sampler.start()
+    times, msv_ms, msv_cells, launches, nhits = [], [], [], 0, 0
+    stage_ms = np.zeros(6)
+    for _ in range(args.steps):
+        flush_l2(torch, l2)
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record()
+        hits, doms = eng.search(ps, ts, cfg)
+        ev1.record()
+        torch.cuda.synchronize()
+        barrier()
+        times.append(ev0.elapsed_time(ev1))
+        st = eng.stats()
+        msv_ms.append(st["ms"][0])
+        msv_cells.append(st["cells"][0])
+        stage_ms += np.array(st["ms"])
+        launches = st["kernel_launches"]
+        nhits = len(hits)
+    clocks = sampler.stop()
+    # ---- end-to-end steps through the C ABI with host buffers ----
+    e2e_times = []
+    h2d = int(seq.nbytes + offs.nbytes + lens.nbytes)
+    d2h = 0
+    pinned = torch.from_numpy(seq).pin_memory().numpy()
+    for _ in range(max(1, args.steps)):
+        flush_l2(torch, l2)
+        barrier()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ts2 = eng.targets_digital(pinned, offs, lens)
+        hits2, doms2 = eng.search(ps, ts2, cfg)
+        ts2.close()
+        torch.cuda.synchronize()
+        e2e_times.append((time.perf_counter() - t) * 1e3)
+        d2h = len(hits2) * 48 + len(doms2) * 56
+    ms_step = max(times) if times else float("nan")
+    e2e_ms = max(e2e_times)
+    if dist is not None:
+        tt = torch.tensor([ms_step, e2e_ms, float(nhits)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_step, e2e_ms = float(tt[0]), float(tt[1])
+    total_cells = cells * ws
+    value = total_cells / (ms_step / 1e3) / 1e9
+    e2e_value = total_cells / (e2e_ms / 1e3) / 1e9
+    # roofline of the dominant kernel (MSV): algorithmic lane-ops per launch / event time
+    msv_t = statistics.median(msv_ms) / 1e3
+    achieved = MSV_OPS_PER_CELL * statistics.median(msv_cells) / msv_t / 1e12
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    peak = 148 * 128 * sm_mhz * 1e6 / 1e12  # FP32 lanes x SMs x sampled SM clock
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "msv_traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get("bytes_per_launch_full")
+        except Exception:
+            traffic = None
+    line = {"metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "profiles_per_rank": int(len(ms)), "targets": int(nt),
+                       "cells_per_rank": cells, "parallelism": f"profile-block x{ws}" if ws > 1 else "single GPU",
+                       "l2": "flushed between steps (256 MiB write)", "calibration": "on device, 200 x L=100 per profile",
+                       "generation_s": round(gen_s, 1), "hits": nhits, "hmm_sha1": sha1(text)},
+            "roofline": {"bound": "alu", "kernel": "msv_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_note": "148 SMs x 128 FP32 lanes x median sampled SM clock (lane-ops/s)"},
+            "stage_ms": [round(x / max(1, args.steps), 3) for x in stage_ms],
+            "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches), "clocks": clocks}
+    if rank == 0 and not args.no_cpu_baseline and ws == 1:
+        line["cpu_baseline"] = {k: v for k, v in cpu_baseline(text, seq, offs, lens, args.cpu_seconds).items()
+                                if k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ps.close()
+    ts.close()
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -92,6 +92,7 @@ def lib():
         "or_results_copy": (None, [P, C.POINTER(OrHit), C.POINTER(OrDom)]),
         "or_results_free": (None, [P]),
         "or_time_pairs": (None, [P, I64, u8, i64p, i64p, C.POINTER(OrCfg), I32, I64, I64, D, i64p, dp, dp, i64p]),
+        "or_score_all": (None, [P, I64, u8, i64p, i64p, I32, fp, fp, fp]),
         "or_decode": (F, [P, I32, u8, I64, I64, I32, fp, fp, fp, fp, fp, fp]),
         "or_viterbi_trace": (I32, [P, I32, u8, I64, C.POINTER(C.c_int32), I32]),
         "or_forward_f64": (D, [P, I32, u8, I64, I32, I32, I64, D]),
@@ -266,6 +267,14 @@ class Oracle:
                             C.byref(nh))
         return dict(pairs=done.value, cells=cells.value, seconds=secs.value, hits=nh.value, threads=nthreads)
 
+    def score_all(self, targets, nthreads=None):
+        """msv, viterbi, forward of every profile x target -> three (P, T) arrays."""
+        n = self.n * targets.n
+        out = [np.zeros(max(n, 1), np.float32) for _ in range(3)]
+        lib().or_score_all(self.h, targets.n, _u8(targets.seq), _i64(targets.offs), _i64(targets.lens),
+                           nthreads or os.cpu_count(), _f(out[0]), _f(out[1]), _f(out[2]))
+        return [o[:n].reshape(self.n, targets.n) for o in out]
+
     def decode(self, i, dsq, l_cfg=None, multihit=True):
         d = np.ascontiguousarray(dsq, np.uint8)
         L = len(d)
@@ -312,6 +321,15 @@ class Oracle:
         pii = np.zeros_like(pm)
         z = lib().or_posterior_f64(self.h, i, _u8(d), L, int(multihit), _d(pm), _d(pii))
         return z, pm.reshape(L + 1, w), pii.reshape(L + 1, w)
+
+
+def calibration_scorer(nthreads=None):
+    """Calibration scorer (see sxhmm.synth.calibrate) backed by the oracle."""
+    def score(profiles, seqs):
+        from sxhmm import synth
+        o = Oracle(text="".join(synth.profile_text(p, cutoffs=False) for p in profiles))
+        return o.score_all(TargetBatch(seqs), nthreads)
+    return score
 
 
 def null_score(l):

@@ -276,6 +276,33 @@ void or_time_pairs(const OrSet* s, int64_t nt, const uint8_t* seq, const int64_t
   *nhits = hitc.load();
 }
 
+// Scores of every profile x every target (profile-major) for calibration:
+// msv, viterbi_score and forward, on `nthreads` threads.
+void or_score_all(const OrSet* s, int64_t nt, const uint8_t* seq, const int64_t* off, const int64_t* len,
+                  int32_t nthreads, float* msv_out, float* vit_out, float* fwd_out) {
+  const int64_t np = (int64_t)s->profiles.size();
+  std::atomic<int64_t> next{0};
+  auto worker = [&]() {
+    DpBuf b;
+    for (;;) {
+      const int64_t idx = next.fetch_add(1);
+      if (idx >= np * nt) break;
+      const int64_t pi = idx / nt, ti = idx % nt;
+      const Profile& p = s->profiles[pi];
+      const uint8_t* d = seq + off[ti];
+      const size_t l = (size_t)len[ti];
+      Xsc xs = Xsc::make(l, true);
+      if (msv_out) msv_out[idx] = msv(p, d, l, b);
+      if (vit_out) vit_out[idx] = viterbi_score(p, d, l, xs, b);
+      if (fwd_out) fwd_out[idx] = forward(p, d, l, xs, b, nullptr);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < std::max(1, nthreads); t++) th.emplace_back(worker);
+  worker();
+  for (auto& t : th) t.join();
+}
+
 // ---- matrices for envelope / posterior checks ----
 // Full-matrix forward+backward+decode of dsq with Xsc(L_cfg, multihit): writes
 // pm, pi ((L+1)*(M+1)) and pn,pj,pc (L+1) and returns the forward score.

@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(256) forward_kernel(
     const int L = tlen[r.t];
     const float4 xs = xsc[r.t];
     const float ploop = xs.z, pmove = xs.w;
-    float* orow = rows ? rows + row_off[w] : nullptr;
+    float* orow = rows ? rows + row_off[in_bins[bin].off + w] : nullptr;
     float mp[VC], ip[VC], dp[VC];
 #pragma unroll
     for (int c = 0; c < VC; c++) mp[c] = ip[c] = dp[c] = 0.f;
@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(256) backward_kernel(
     const int L = tlen[r.t];
     const float4 xs = xsc[r.t];
     const float ploop = xs.z, pmove = xs.w;
-    float* orow = rows + row_off[w];
+    float* orow = rows + row_off[in_bins[bin].off + w];
     float mn[VC], in_[VC], dn[VC];
     // row L
     float xc = pmove;

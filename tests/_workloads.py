@@ -23,19 +23,7 @@ def fixture_targets():
     return O.read_fasta(os.path.join(GOLDEN, "hmmer34_targets.faa"))
 
 
-def oracle_scorer(profiles, seqs):
-    """Calibration scorer backed by the oracle (tests only)."""
-    text = "".join(synth.profile_text(p) for p in profiles)
-    o = O.Oracle(text=text)
-    msv = np.zeros((len(profiles), len(seqs)))
-    vit = np.zeros_like(msv)
-    fwd = np.zeros_like(msv)
-    for i in range(len(profiles)):
-        for j, s in enumerate(seqs):
-            msv[i, j] = o.msv(i, s)
-            vit[i, j] = o.viterbi(i, s)
-            fwd[i, j] = o.forward(i, s)
-    return msv, vit, fwd
+oracle_scorer = O.calibration_scorer()
 
 
 @functools.lru_cache(maxsize=None)

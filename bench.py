@@ -221,7 +221,8 @@ def main():
     sampler = ClockSampler(local)
     sampler.start()
     times, msv_ms, msv_cells, launches, nhits = [], [], [], 0, 0
-    stage_ms = np.zeros(6)
+    stage_ms = np.zeros(8)
+    stage_pairs = None
     for _ in range(args.steps):
         flush_l2(torch, l2)
         barrier()
@@ -237,6 +238,7 @@ def main():
         msv_cells.append(st["cells"][0])
         stage_ms += np.array(st["ms"])
         launches = st["kernel_launches"]
+        stage_pairs = st["pairs_in"][:6]
         nhits = len(hits)
     clocks = sampler.stop()
     # ---- end-to-end steps through the C ABI with host buffers ----
@@ -286,7 +288,9 @@ def main():
             "roofline": {"bound": "alu", "kernel": "msv_kernel", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_note": "148 SMs x 128 FP32 lanes x median sampled SM clock (lane-ops/s)"},
-            "stage_ms": [round(x / max(1, args.steps), 3) for x in stage_ms],
+            "stage_ms": {k: round(v / max(1, args.steps), 3) for k, v in zip(
+                ["msv", "bias", "viterbi", "forward", "rows", "host_domains", "total"], stage_ms)},
+            "stage_pairs_in": dict(zip(["msv", "bias", "viterbi", "forward", "rows", "host_domains"], stage_pairs or [])),
             "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches), "clocks": clocks}
     if rank == 0 and not args.no_cpu_baseline and ws == 1:

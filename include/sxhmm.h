@@ -147,13 +147,14 @@ const sx_domain* sx_hits_domains(const sx_hits* h);
 void sx_hits_free(sx_hits* h);
 
 /* Per-stage counters of the last sx_search on this engine: pairs entering and
- * leaving each stage, DP cells per stage and device milliseconds per stage.
- * stage: 0 MSV, 1 bias, 2 Viterbi, 3 Forward pre-screen, 4 Forward/Backward
- * rows, 5 host domain definition. */
+ * leaving each stage, DP cells per stage and milliseconds per stage.
+ * stage: 0 MSV, 1 bias, 2 Viterbi, 3 Forward pre-screen (device, CUDA
+ * events), 4 Forward/Backward row passes of the final pairs (device + copies),
+ * 5 host domain definition, 6 whole call (host clock). */
 typedef struct {
-  int64_t pairs_in[6], pairs_out[6];
-  double cells[6];
-  double ms[6];
+  int64_t pairs_in[8], pairs_out[8];
+  double cells[8];
+  double ms[8];
   int64_t kernel_launches;
 } sx_search_stats;
 int sx_last_search_stats(const sx_engine* e, sx_search_stats* out);

@@ -93,10 +93,13 @@ struct DevBuf {
 struct MsvShape {
   int g, c;
 };
-constexpr MsvShape kMsvShapes[] = {{1, 8},  {1, 16},  {1, 24},  {1, 32},  {2, 8},   {2, 16},  {2, 24},
-                                   {2, 32}, {4, 8},   {4, 16},  {4, 24},  {4, 32},  {8, 8},   {8, 16},
-                                   {8, 24}, {8, 32},  {16, 8},  {16, 16}, {16, 24}, {16, 32}, {32, 8},
-                                   {32, 16}, {32, 24}, {32, 32}, {32, 48}, {32, 64}};
+constexpr MsvShape kMsvShapes[] = {
+    {1, 8}, {1, 16}, {1, 24}, {1, 32}, {1, 40}, {1, 48}, {1, 56}, {1, 64},
+    {2, 8}, {2, 16}, {2, 24}, {2, 32}, {2, 40}, {2, 48}, {2, 56}, {2, 64},
+    {4, 8}, {4, 16}, {4, 24}, {4, 32}, {4, 40}, {4, 48}, {4, 56}, {4, 64},
+    {8, 8}, {8, 16}, {8, 24}, {8, 32}, {8, 40}, {8, 48}, {8, 56}, {8, 64},
+    {16, 8}, {16, 16}, {16, 24}, {16, 32}, {16, 40}, {16, 48}, {16, 56}, {16, 64},
+    {32, 8}, {32, 16}, {32, 24}, {32, 32}, {32, 40}, {32, 48}, {32, 56}, {32, 64}};
 constexpr int kNumMsvShapes = sizeof(kMsvShapes) / sizeof(kMsvShapes[0]);
 constexpr int kMaxM = 2048;
 // Warp-chunked column counts (columns per lane, 32 lanes per pair).
@@ -155,18 +158,20 @@ const KernelTables& kernels() {
   return t;
 }
 
-// Pick the MSV shape with the fewest estimated issued instructions per useful
-// DP cell: per row a warp issues ~(2.6C + 2log2(G) + 17) instructions and
-// advances 32/G targets by M cells each.
+// Pick the MSV shape with the fewest issued instructions per useful DP cell.
+// Per row a warp issues about 2.75*C instructions of cell work (FADD, FMNMX,
+// a share of FMNMX3 and LDS.128) plus ~44 of per-row overhead (residue
+// extraction, shuffles, specials) and 2 per butterfly step; it advances 32/G
+// targets by M cells each (fitted to ncu instruction counts on B200).
 int choose_msv_shape(int m) {
   int best = -1;
   double best_cost = 1e30;
   for (int s = 0; s < kNumMsvShapes; s++) {
     const int g = kMsvShapes[s].g, c = kMsvShapes[s].c;
     if (g * c < m) continue;
-    const double instr = 2.6 * c + 2.0 * std::log2((double)g) + 17.0;
+    const double instr = 2.75 * c + 44.0 + 2.0 * std::log2((double)g);
     const double cost = instr / ((32.0 / g) * m);
-    if (cost < best_cost) {
+    if (cost < best_cost * 0.999) {
       best_cost = cost;
       best = s;
     }
@@ -243,9 +248,13 @@ struct sx_engine {
   int64_t batch_bytes = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
+  static constexpr int kAux = 8;
+  cudaStream_t aux[kAux] = {};  // independent launches (shapes, bins) run side by side
+  cudaEvent_t fork_ev = nullptr, join_ev[kAux] = {};
   cudaEvent_t ev[8] = {};
   std::mutex mu;
   sx_search_stats stats{};
+  double host_ms = 0;  // host time inside rows_pass sinks (domain definition)
   // grow-only device scratch
   DevBuf<PairRec> lists[4];
   DevBuf<BinRegion> bins[4];
@@ -292,6 +301,19 @@ struct sx_hits {
 };
 
 namespace {
+
+// Fan independent launches out over the auxiliary streams and join them back
+// into the engine stream.
+void fork_aux(sx_engine* E) {
+  CK(cudaEventRecord(E->fork_ev, E->stream));
+  for (int a = 0; a < sx_engine::kAux; a++) CK(cudaStreamWaitEvent(E->aux[a], E->fork_ev, 0));
+}
+void join_aux(sx_engine* E) {
+  for (int a = 0; a < sx_engine::kAux; a++) {
+    CK(cudaEventRecord(E->join_ev[a], E->aux[a]));
+    CK(cudaStreamWaitEvent(E->stream, E->join_ev[a], 0));
+  }
+}
 
 // ---- profile packing --------------------------------------------------------
 void pack_profiles(sx_profiles* P) {
@@ -566,25 +588,30 @@ void rows_pass(sx_engine* E, const sx_profiles* P, const sx_targets* T, const st
     // rows the kernels never touch are zero
     CK(cudaMemsetAsync(E->rows_f.p, 0, sizeof(float) * (size_t)ro, s));
     CK(cudaMemsetAsync(E->rows_b.p, 0, sizeof(float) * (size_t)ro, s));
+    fork_aux(E);
     for (int b = 0; b < kNumVbins; b++) {
       if (!cnt[b]) continue;
       const int blocks = (int)std::min<int64_t>((cnt[b] + 7) / 8, (int64_t)E->num_sms * 16);
-      K.fwd[b]<<<blocks, 256, 0, s>>>(E->lists[3].p, E->counts.p + 3 * kNumVbins, E->bins[3].p, b, nullptr, nullptr,
-                                      nullptr, E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p,
-                                      T->d_off.p, T->d_len.p, T->d_xsc.p, 0.f, E->rows_f.p, E->row_off.p);
-      K.bwd[b]<<<blocks, 256, 0, s>>>(E->lists[3].p, E->counts.p + 3 * kNumVbins, E->bins[3].p, b, P->d_prof.p,
-                                      P->d_vfb.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p, E->rows_b.p,
-                                      E->row_off.p);
+      cudaStream_t sa = E->aux[(2 * b) % sx_engine::kAux], sb = E->aux[(2 * b + 1) % sx_engine::kAux];
+      K.fwd[b]<<<blocks, 256, 0, sa>>>(E->lists[3].p, E->counts.p + 3 * kNumVbins, E->bins[3].p, b, nullptr, nullptr,
+                                       nullptr, E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p,
+                                       T->d_off.p, T->d_len.p, T->d_xsc.p, 0.f, E->rows_f.p, E->row_off.p);
+      K.bwd[b]<<<blocks, 256, 0, sb>>>(E->lists[3].p, E->counts.p + 3 * kNumVbins, E->bins[3].p, b, P->d_prof.p,
+                                       P->d_vfb.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p, E->rows_b.p,
+                                       E->row_off.p);
       E->stats.kernel_launches += 2;
     }
     CK(cudaGetLastError());
+    join_aux(E);
     std::vector<float> hf((size_t)ro), hb((size_t)ro);
     CK(cudaMemcpyAsync(hf.data(), E->rows_f.p, sizeof(float) * (size_t)ro, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(hb.data(), E->rows_b.p, sizeof(float) * (size_t)ro, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    const auto t_host = std::chrono::steady_clock::now();
     parallel_for(which.size(), E->host_threads, [&](size_t q) {
       sink(which[q], hf.data() + roff[q], hb.data() + roff[q]);
     });
+    E->host_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host).count();
     i0 = i1;
   }
 }
@@ -709,18 +736,28 @@ void launch_msv(sx_engine* E, const sx_profiles* P, const sx_targets* T, const s
   start[kNumMsvShapes] = all.size();
   if (all.empty()) return;
   E->tiles.upload(all.data(), all.size(), E->stream);
-  for (int s = 0; s < kNumMsvShapes; s++) {
+  // biggest launches first, each on its own auxiliary stream
+  std::vector<int> order;
+  for (int s = 0; s < kNumMsvShapes; s++)
+    if (start[s + 1] > start[s]) order.push_back(s);
+  std::vector<double> work(kNumMsvShapes, 0.0);
+  for (int s : order)
+    for (size_t q = start[s]; q < start[s + 1]; q++) work[s] += (double)all[q].end - all[q].begin;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+  fork_aux(E);
+  int lane = 0;
+  for (int s : order) {
     const size_t nt = start[s + 1] - start[s];
-    if (!nt) continue;
     const int g = kMsvShapes[s].g, c = kMsvShapes[s].c;
     const size_t smem = 25ull * (c / 4) * g * sizeof(float4);
     CK(cudaFuncSetAttribute((const void*)K.msv[s], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    K.msv[s]<<<(unsigned)nt, 256, smem, E->stream>>>(E->tiles.p + start[s], P->d_prof.p, E->thr.p, P->d_msv.p,
-                                                     T->d_res.p, T->d_off.p, T->d_len.p, T->d_tpar.p, d_list,
-                                                     d_scores, d_slot, surv, bins, counts, E->overflow.p);
+    K.msv[s]<<<(unsigned)nt, 256, smem, E->aux[lane++ % sx_engine::kAux]>>>(
+        E->tiles.p + start[s], P->d_prof.p, E->thr.p, P->d_msv.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_tpar.p,
+        d_list, d_scores, d_slot, surv, bins, counts, E->overflow.p);
     E->stats.kernel_launches++;
   }
   CK(cudaGetLastError());
+  join_aux(E);
 }
 
 // One filter stage over per-vbin lists: stage `si` reads lists[si] and writes lists[si+1].
@@ -739,9 +776,12 @@ void launch_stage(sx_engine* E, const sx_profiles* P, const sx_targets* T, int s
                                           kSlackBits, nullptr);
     E->stats.kernel_launches++;
   } else {
+    fork_aux(E);
+    int lane = 0;
     for (int b = 0; b < kNumVbins; b++) {
       if (!nin[b]) continue;
       const int blocks = (int)std::min<int64_t>((nin[b] + 7) / 8, (int64_t)E->num_sms * 16);
+      cudaStream_t s = E->aux[lane++ % sx_engine::kAux];
       if (si == 1)
         K.vit[b]<<<blocks, 256, 0, s>>>(E->lists[1].p, cin, E->bins[1].p, b, E->lists[2].p, E->bins[2].p, cout,
                                         E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
@@ -752,6 +792,7 @@ void launch_stage(sx_engine* E, const sx_profiles* P, const sx_targets* T, int s
                                         T->d_len.p, T->d_xsc.p, kSlackBits, nullptr, nullptr);
       E->stats.kernel_launches++;
     }
+    join_aux(E);
   }
   CK(cudaGetLastError());
 }
@@ -766,6 +807,7 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
   int rc = check_cutoffs(P, cfg->cutoff_kind);
   if (rc) return rc;
   E->stats = sx_search_stats{};
+  E->host_ms = 0;
   SearchOpts o;
   o.filters = cfg->filters != 0;
   o.null2 = cfg->null2 != 0;
@@ -905,9 +947,12 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
   });
   auto t_end = std::chrono::steady_clock::now();
   E->stats.pairs_out[4] = n_domain.load();
-  E->stats.ms[4] = std::chrono::duration<double, std::milli>(t_end - t_rows).count();
+  const double rows_total = std::chrono::duration<double, std::milli>(t_end - t_rows).count();
+  E->stats.ms[4] = rows_total - E->host_ms;
+  E->stats.ms[5] = E->host_ms;
+  E->stats.pairs_in[5] = n_domain.load();
   for (const auto& f : finals) E->stats.cells[4] += (double)P->h[f.p].m * T->len[f.t];
-  E->stats.ms[5] = std::chrono::duration<double, std::milli>(t_end - t_start).count();
+  E->stats.ms[6] = std::chrono::duration<double, std::milli>(t_end - t_start).count();
   std::vector<std::vector<std::pair<int32_t, HitOut>>> per(np);
   for (size_t i = 0; i < finals.size(); i++)
     if (res[i].hit) per[finals[i].p].emplace_back(finals[i].t, std::move(res[i].h));
@@ -945,6 +990,11 @@ int sx_create(const sx_opts* opts, sx_engine** out) {
     e->num_sms = prop.multiProcessorCount;
     CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     for (auto& ev : e->ev) CK(cudaEventCreate(&ev));
+    for (int a = 0; a < sx_engine::kAux; a++) {
+      CK(cudaStreamCreateWithFlags(&e->aux[a], cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&e->join_ev[a], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming));
     (void)kernels();
   } catch (const CudaError& ce) {
     return fail(ce.code, ce.msg);
@@ -959,6 +1009,11 @@ void sx_destroy(sx_engine* e) {
   if (e->stream) cudaStreamSynchronize(e->stream);
   for (auto& ev : e->ev)
     if (ev) cudaEventDestroy(ev);
+  for (int a = 0; a < sx_engine::kAux; a++) {
+    if (e->aux[a]) cudaStreamDestroy(e->aux[a]);
+    if (e->join_ev[a]) cudaEventDestroy(e->join_ev[a]);
+  }
+  if (e->fork_ev) cudaEventDestroy(e->fork_ev);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }

@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
                                                   float* __restrict__ score_out, const int32_t* __restrict__ slot,
                                                   PairRec* __restrict__ surv, const BinRegion* __restrict__ bins,
                                                   unsigned* __restrict__ counts, unsigned* __restrict__ overflow) {
-  static_assert(C % 4 == 0 && (G & (G - 1)) == 0 && G <= 32, "bad MSV shape");
+  static_assert(C % 8 == 0 && (G & (G - 1)) == 0 && G <= 32, "bad MSV shape");
   constexpr int NC4 = C / 4;
   constexpr int ROW4 = NC4 * G;  // float4 per residue row
   extern __shared__ float4 sm_rows[];
@@ -172,6 +172,7 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
     if (__all_sync(kFull, done)) break;
 
     const int q = (row - boff) >> 2;
+    const int rem = L - row;  // rows left in the target; the score is latched when it reaches 0
     uint32_t w = q == 0 ? rcur.x : q == 1 ? rcur.y : q == 2 ? rcur.z : rcur.w;
     if (done) w = 0x18181818u;  // '*' rows: all -inf, never read back
 #pragma unroll
@@ -184,34 +185,31 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
       const float be = fadd(xb, tbm);
       float left = __shfl_up_sync(kFull, prev[C - 1], 1, G);
       if (j == 0) left = SX_NEG_INF;
-      float xe = SX_NEG_INF;
+      // new row in place, highest column first so prev[c-1] is still the old value
 #pragma unroll
-      for (int c = C - 1; c >= 1; c -= 2) {
+      for (int c = C - 1; c >= 1; c--) {
         const float4& a4 = rv[c >> 2];
         const float ra = (c & 3) == 0 ? a4.x : (c & 3) == 1 ? a4.y : (c & 3) == 2 ? a4.z : a4.w;
-        const float va = fadd(ra, fmx(prev[c - 1], be));
-        prev[c] = va;
-        if (c - 1 >= 1) {
-          const int cb = c - 1;
-          const float4& b4 = rv[cb >> 2];
-          const float rb = (cb & 3) == 0 ? b4.x : (cb & 3) == 1 ? b4.y : (cb & 3) == 2 ? b4.z : b4.w;
-          const float vb = fadd(rb, fmx(prev[cb - 1], be));
-          prev[cb] = vb;
-          xe = fmx3(xe, va, vb);
-        } else {
-          xe = fmx(xe, va);
-        }
+        prev[c] = fadd(ra, fmx(prev[c - 1], be));
       }
-      const float v0 = fadd(rv[0].x, fmx(left, be));
-      prev[0] = v0;
-      xe = fmx(xe, v0);
+      prev[0] = fadd(rv[0].x, fmx(left, be));
+      // row maximum: a depth-3 tree of 3-input maxes per 8 columns
+      float blk[C / 8];
+#pragma unroll
+      for (int b = 0; b < C / 8; b++) {
+        const float* v = prev + 8 * b;
+        blk[b] = fmx3(fmx3(v[0], v[1], v[2]), fmx3(v[3], v[4], v[5]), fmx(v[6], v[7]));
+      }
+      float xe = blk[0];
+#pragma unroll
+      for (int b = 1; b < C / 8; b += 2) xe = (b + 1 < C / 8) ? fmx3(xe, blk[b], blk[b + 1]) : fmx(xe, blk[b]);
 #pragma unroll
       for (int o = G / 2; o >= 1; o >>= 1) xe = fmx(xe, __shfl_xor_sync(kFull, xe, o, G));
       xj = fmx(fadd(xj, tloop), fadd(xe, -kLn2));
       xc = fmx(fadd(xc, tloop), fadd(xe, -kLn2));
       xn = fadd(xn, tloop);
       xb = fmx(fadd(xn, tmove), fadd(xj, tmove));
-      if (row + r + 1 == L) fin = fadd(xc, tmove);
+      if (rem == r + 1) fin = fadd(xc, tmove);
     }
     row += 4;
     if (row - boff == 16) {
@@ -279,6 +277,28 @@ struct Img {
   __device__ __forceinline__ float at(int row, int c, int lane) const { return __ldg(base + ((row * VC + c) << 5) + lane); }
 };
 
+// Eight per-column transition rows of the image starting at `row0`: held in
+// registers for the whole pair when VC is small (M <= 128), re-read from the
+// (L1-cached) image otherwise.
+template <int VC, bool kHold = (VC <= 4)>
+struct TransRows {
+  float t[8][VC];
+  __device__ __forceinline__ void load(const Img<VC>& img, int row0, int lane) {
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+#pragma unroll
+      for (int c = 0; c < VC; c++) t[q][c] = img.at(row0 + q, c, lane);
+  }
+  __device__ __forceinline__ float get(const Img<VC>&, int, int q, int c, int) const { return t[q][c]; }
+};
+template <int VC>
+struct TransRows<VC, false> {
+  __device__ __forceinline__ void load(const Img<VC>&, int, int) {}
+  __device__ __forceinline__ float get(const Img<VC>& img, int row0, int q, int c, int lane) const {
+    return img.at(row0 + q, c, lane);
+  }
+};
+
 // ===========================================================================
 // Viterbi filter (src/hmmer/dp.rs:152-189), one warp per pair, lane l holding
 // columns l*VC+1 .. l*VC+VC.  M and I cells of a row are independent; the
@@ -305,12 +325,21 @@ __global__ void __launch_bounds__(256) viterbi_kernel(
     const uint8_t* s = res + toff[r.t];
     const int L = tlen[r.t];
     const float4 xs = xsc[r.t];  // loop, move (log), ploop, pmove
-    float mp[VC], ip[VC], dp[VC];
+    TransRows<VC> tr;
+    tr.load(img, kRowVit, lane);
+    float mp[VC], ip[VC], dp[VC], rs[VC];
 #pragma unroll
     for (int c = 0; c < VC; c++) mp[c] = ip[c] = dp[c] = SX_NEG_INF;
     float xn = 0.f, xb = xs.y, xj = SX_NEG_INF, xc = SX_NEG_INF;
+    int x = L > 0 ? __ldg(s) : 24;
+#pragma unroll
+    for (int c = 0; c < VC; c++) rs[c] = img.at(kRowMsc + x, c, lane);
     for (int i = 0; i < L; i++) {
-      const int x = __ldg(s + i);
+      // prefetch the next row's residue and match scores
+      const int xnext = (i + 1 < L) ? __ldg(s + i + 1) : 24;
+      float rsn[VC];
+#pragma unroll
+      for (int c = 0; c < VC; c++) rsn[c] = img.at(kRowMsc + xnext, c, lane);
       const bool ins_ok = x != 24;
       const float mpl0 = __shfl_up_sync(kFull, mp[VC - 1], 1);
       const float ipl0 = __shfl_up_sync(kFull, ip[VC - 1], 1);
@@ -321,11 +350,12 @@ __global__ void __launch_bounds__(256) viterbi_kernel(
       for (int c = 0; c < VC; c++) {
         const int k = lane * VC + c + 1;
         const float mpv = c ? mp[c - 1] : mpl, ipv = c ? ip[c - 1] : ipl, dpv = c ? dp[c - 1] : dpl;
-        const float sc = fmx(fmx(fadd(mpv, img.at(kRowVit + 0, c, lane)), fadd(ipv, img.at(kRowVit + 1, c, lane))),
-                             fmx(fadd(xb, img.at(kRowVit + 3, c, lane)), fadd(dpv, img.at(kRowVit + 2, c, lane))));
-        mv[c] = fadd(sc, img.at(kRowMsc + x, c, lane));
-        iv[c] = (k < M && ins_ok) ? fmx(fadd(mp[c], img.at(kRowVit + 4, c, lane)), fadd(ip[c], img.at(kRowVit + 5, c, lane)))
-                                  : SX_NEG_INF;
+        const float sc = fmx(fmx(fadd(mpv, tr.get(img, kRowVit, 0, c, lane)), fadd(ipv, tr.get(img, kRowVit, 1, c, lane))),
+                             fmx(fadd(xb, tr.get(img, kRowVit, 3, c, lane)), fadd(dpv, tr.get(img, kRowVit, 2, c, lane))));
+        mv[c] = fadd(sc, rs[c]);
+        iv[c] = (k < M && ins_ok)
+                    ? fmx(fadd(mp[c], tr.get(img, kRowVit, 4, c, lane)), fadd(ip[c], tr.get(img, kRowVit, 5, c, lane)))
+                    : SX_NEG_INF;
       }
       // D chain, first pass with carry -inf
       const float mcl0 = __shfl_up_sync(kFull, mv[VC - 1], 1);
@@ -333,7 +363,7 @@ __global__ void __launch_bounds__(256) viterbi_kernel(
 #pragma unroll
       for (int c = 0; c < VC; c++) {
         const float mcv = c ? mv[c - 1] : (lane ? mcl0 : SX_NEG_INF);
-        d = fmx(fadd(mcv, img.at(kRowVit + 6, c, lane)), fadd(d, img.at(kRowVit + 7, c, lane)));
+        d = fmx(fadd(mcv, tr.get(img, kRowVit, 6, c, lane)), fadd(d, tr.get(img, kRowVit, 7, c, lane)));
         dv[c] = d;
       }
       // push carries across lanes until nothing changes (at most 31 rounds)
@@ -344,7 +374,7 @@ __global__ void __launch_bounds__(256) viterbi_kernel(
 #pragma unroll
         for (int c = 0; c < VC; c++) {
           if (go) {
-            const float cand = fadd(cin, img.at(kRowVit + 7, c, lane));
+            const float cand = fadd(cin, tr.get(img, kRowVit, 7, c, lane));
             if (cand > dv[c]) {
               dv[c] = cand;
               cin = cand;
@@ -370,7 +400,9 @@ __global__ void __launch_bounds__(256) viterbi_kernel(
         mp[c] = mv[c];
         ip[c] = iv[c];
         dp[c] = dv[c];
+        rs[c] = rsn[c];
       }
+      x = xnext;
     }
     const float vsc = (L > 0 && M > 0) ? fadd(xc, xs.y) : SX_NEG_INF;
     if (lane == 0) {
@@ -412,13 +444,21 @@ __global__ void __launch_bounds__(256) forward_kernel(
     const float4 xs = xsc[r.t];
     const float ploop = xs.z, pmove = xs.w;
     float* orow = rows ? rows + row_off[in_bins[bin].off + w] : nullptr;
-    float mp[VC], ip[VC], dp[VC];
+    TransRows<VC> tr;
+    tr.load(img, kRowFwd, lane);
+    float mp[VC], ip[VC], dp[VC], eo[VC];
 #pragma unroll
     for (int c = 0; c < VC; c++) mp[c] = ip[c] = dp[c] = 0.f;
     float xn = 1.f, xb = pmove, xj = 0.f, xc = 0.f;
     double lnscale = 0.0;
+    int x = L > 0 ? __ldg(s) : 24;
+#pragma unroll
+    for (int c = 0; c < VC; c++) eo[c] = img.at(kRowMo + x, c, lane);
     for (int i = 0; i < L; i++) {
-      const int x = __ldg(s + i);
+      const int xnext = (i + 1 < L) ? __ldg(s + i + 1) : 24;
+      float eon[VC];
+#pragma unroll
+      for (int c = 0; c < VC; c++) eon[c] = img.at(kRowMo + xnext, c, lane);
       const float ins = x != 24 ? 1.f : 0.f;
       const float mpl0 = __shfl_up_sync(kFull, mp[VC - 1], 1);
       const float ipl0 = __shfl_up_sync(kFull, ip[VC - 1], 1);
@@ -429,20 +469,20 @@ __global__ void __launch_bounds__(256) forward_kernel(
       for (int c = 0; c < VC; c++) {
         const int k = lane * VC + c + 1;
         const float mpv = c ? mp[c - 1] : mpl, ipv = c ? ip[c - 1] : ipl, dpv = c ? dp[c - 1] : dpl;
-        float t = fmul(xb, img.at(kRowFwd + 0, c, lane));
-        t = fadd(t, fmul(mpv, img.at(kRowFwd + 1, c, lane)));
-        t = fadd(t, fmul(ipv, img.at(kRowFwd + 2, c, lane)));
-        t = fadd(t, fmul(dpv, img.at(kRowFwd + 3, c, lane)));
-        mv[c] = fmul(t, img.at(kRowMo + x, c, lane));
-        iv[c] = k < M ? fmul(fadd(fmul(mp[c], img.at(kRowFwd + 4, c, lane)), fmul(ip[c], img.at(kRowFwd + 5, c, lane))), ins)
+        float t = fmul(xb, tr.get(img, kRowFwd, 0, c, lane));
+        t = fadd(t, fmul(mpv, tr.get(img, kRowFwd, 1, c, lane)));
+        t = fadd(t, fmul(ipv, tr.get(img, kRowFwd, 2, c, lane)));
+        t = fadd(t, fmul(dpv, tr.get(img, kRowFwd, 3, c, lane)));
+        mv[c] = fmul(t, eo[c]);
+        iv[c] = k < M ? fmul(fadd(fmul(mp[c], tr.get(img, kRowFwd, 4, c, lane)), fmul(ip[c], tr.get(img, kRowFwd, 5, c, lane))), ins)
                       : 0.f;
       }
       const float mcl0 = __shfl_up_sync(kFull, mv[VC - 1], 1);
       const float mcl = lane ? mcl0 : 0.f;
 #pragma unroll
       for (int c = 0; c < VC; c++) {
-        a[c] = fmul(c ? mv[c - 1] : mcl, img.at(kRowFwd + 6, c, lane));
-        pdd[c] = img.at(kRowFwd + 7, c, lane);
+        a[c] = fmul(c ? mv[c - 1] : mcl, tr.get(img, kRowFwd, 6, c, lane));
+        pdd[c] = tr.get(img, kRowFwd, 7, c, lane);
       }
       // ordered D chain and row sum: dc[k] = a_k + dc[k-1]*p_dd[k-1]; xe += mv + dc
       float dcar = 0.f, xe = 0.f;
@@ -493,7 +533,9 @@ __global__ void __launch_bounds__(256) forward_kernel(
         mp[c] = mv[c];
         ip[c] = iv[c];
         dp[c] = dv[c];
+        eo[c] = eon[c];
       }
+      x = xnext;
     }
     if (lane == 0) {
       const float v = fmul(xc, pmove);

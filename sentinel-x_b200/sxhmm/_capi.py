@@ -46,8 +46,8 @@ class SxProfileInfo(C.Structure):
 
 
 class SxSearchStats(C.Structure):
-    _fields_ = [("pairs_in", C.c_int64 * 6), ("pairs_out", C.c_int64 * 6), ("cells", C.c_double * 6),
-                ("ms", C.c_double * 6), ("kernel_launches", C.c_int64)]
+    _fields_ = [("pairs_in", C.c_int64 * 8), ("pairs_out", C.c_int64 * 8), ("cells", C.c_double * 8),
+                ("ms", C.c_double * 8), ("kernel_launches", C.c_int64)]
 
 
 _i32p = C.POINTER(C.c_int32)

@@ -184,6 +184,23 @@ int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, c
                       const int32_t* pair_target, size_t npairs, int32_t m, float* d_msc, float* d_isc,
                       float* d_trans, double* lnz);
 
+/* ---- scoring without allocation ----------------------------------------- */
+/* No counterpart in the reference.  Viterbi scores (as sx_score_pairs computes
+ * them) for up to 8192 pairs per call, for callers that must not allocate GPU
+ * memory during the call: for example a host program that shares the GPU with
+ * another runtime whose caching allocator already holds nearly all device
+ * memory, or a latency-bound caller that cannot absorb the device-wide
+ * synchronisation a cudaMalloc/cudaFree can imply.  Instead of engine scratch
+ * it uses one fixed device array of about 360 KB that every GPU holding this
+ * library keeps reserved until the process exits.  The first call on a device
+ * looks up that array's device address; make that first call before any
+ * stream capture begins on the device.  More than 8192 pairs is an SX_EINVAL
+ * error.  All calls on a device share the array: calls that overlap on the
+ * GPU (for example from two engines on one device) race; calls on one engine
+ * are serialised.  Inputs and outputs are host arrays, as for sx_score_pairs. */
+int sx_score_viterbi_static(sx_engine* e, const sx_profiles* p, const sx_targets* t, const int32_t* pair_profile,
+                            const int32_t* pair_target, size_t npairs, float* viterbi);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,6 +79,7 @@ SIGNATURES = {
     "sx_last_search_stats": (C.c_int, [_P, C.POINTER(SxSearchStats)]),
     "sx_score_pairs": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, _fp, _fp, _fp, _fp, _fp]),
     "sx_posterior_grad": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, C.c_int32, _fp, _fp, _fp, _dp]),
+    "sx_score_viterbi_static": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, _fp]),
 }
 
 

@@ -33,6 +33,7 @@
 #include "../../include/sxhmm.h"
 #include "internal.hpp"
 #include "kernels.cuh"
+#include "adjoint.cuh"
 
 using namespace sx;
 using sxk::BinRegion;
@@ -117,6 +118,10 @@ typedef void (*FwdFn)(const PairRec*, const unsigned*, const BinRegion*, int, Pa
                       const int32_t*, const float4*, float, float*, const int64_t*);
 typedef void (*BwdFn)(const PairRec*, const unsigned*, const BinRegion*, int, const DevProfile*, const float*,
                       const uint8_t*, const int64_t*, const int32_t*, const float4*, float*, const int64_t*);
+typedef void (*AdjFFn)(const sxk::AdjPair*, int, const DevProfile*, const float*, const uint8_t*, const int64_t*,
+                       const int32_t*, const float4*, float*, double*, double*);
+typedef void (*AdjBFn)(const sxk::AdjPair*, int, const DevProfile*, const float*, const uint8_t*, const int64_t*,
+                       const int32_t*, const float4*, float*, const double*, const double*, float*);
 
 template <int I>
 struct MsvTable {
@@ -131,16 +136,18 @@ struct MsvTable<kNumMsvShapes> {
 };
 template <int I>
 struct VbinTable {
-  static void fill(VitFn* v, FwdFn* f, BwdFn* b) {
+  static void fill(VitFn* v, FwdFn* f, BwdFn* b, AdjFFn* af, AdjBFn* ab) {
     v[I] = sxk::viterbi_kernel<kVcBins[I]>;
     f[I] = sxk::forward_kernel<kVcBins[I]>;
     b[I] = sxk::backward_kernel<kVcBins[I]>;
-    VbinTable<I + 1>::fill(v, f, b);
+    af[I] = sxk::adjoint_forward_kernel<kVcBins[I]>;
+    ab[I] = sxk::adjoint_backward_kernel<kVcBins[I]>;
+    VbinTable<I + 1>::fill(v, f, b, af, ab);
   }
 };
 template <>
 struct VbinTable<kNumVbins> {
-  static void fill(VitFn*, FwdFn*, BwdFn*) {}
+  static void fill(VitFn*, FwdFn*, BwdFn*, AdjFFn*, AdjBFn*) {}
 };
 
 struct KernelTables {
@@ -148,9 +155,11 @@ struct KernelTables {
   VitFn vit[kNumVbins];
   FwdFn fwd[kNumVbins];
   BwdFn bwd[kNumVbins];
+  AdjFFn adjf[kNumVbins];
+  AdjBFn adjb[kNumVbins];
   KernelTables() {
     MsvTable<0>::fill(msv);
-    VbinTable<0>::fill(vit, fwd, bwd);
+    VbinTable<0>::fill(vit, fwd, bwd, adjf, adjb);
   }
 };
 const KernelTables& kernels() {
@@ -266,6 +275,9 @@ struct sx_engine {
   DevBuf<int64_t> row_off;
   DevBuf<float> scores;
   DevBuf<int32_t> slots, plist;
+  DevBuf<sxk::AdjPair> adj_pairs;
+  DevBuf<float> adj_f;
+  DevBuf<double> adj_d, adj_lnz;
 };
 
 struct sx_profiles {
@@ -1285,9 +1297,83 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
 int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, const int32_t* pair_profile,
                       const int32_t* pair_target, size_t npairs, int32_t m, float* d_msc, float* d_isc,
                       float* d_trans, double* lnz) {
-  (void)e; (void)p; (void)t; (void)pair_profile; (void)pair_target; (void)npairs; (void)m;
-  (void)d_msc; (void)d_isc; (void)d_trans; (void)lnz;
-  return fail(SX_EINVAL, "sx_posterior_grad: not available in this build");
+  if (!e || !p || !t || (npairs && (!pair_profile || !pair_target || !d_msc || !d_isc || !d_trans || !lnz)))
+    return fail(SX_EINVAL, "sx_posterior_grad: NULL argument");
+  std::lock_guard<std::mutex> lk(e->mu);
+  const size_t np = p->h.size(), nt = t->len.size();
+  for (size_t i = 0; i < npairs; i++) {
+    if (pair_profile[i] < 0 || (size_t)pair_profile[i] >= np || pair_target[i] < 0 || (size_t)pair_target[i] >= nt)
+      return fail(SX_EINVAL, "sx_posterior_grad: pair " + std::to_string(i) + " out of range");
+    if (p->h[pair_profile[i]].m != m)
+      return fail(SX_EINVAL, "sx_posterior_grad: pair " + std::to_string(i) + " uses a profile of M=" +
+                                 std::to_string(p->h[pair_profile[i]].m) + ", expected " + std::to_string(m));
+  }
+  if (!npairs) return SX_OK;
+  const int W = m + 1;
+  const size_t out_per = (size_t)(25 + 25 + 8) * W;
+  try {
+    CK(cudaSetDevice(e->device));
+    cudaStream_t s = e->stream;
+    const int vb = p->dp[pair_profile[0]].vbin, VC = kVcBins[vb];
+    const auto& K = kernels();
+    const int64_t budget = std::max<int64_t>(e->batch_bytes, 64LL << 20);
+    std::vector<float> host_out;
+    size_t i0 = 0;
+    while (i0 < npairs) {
+      // chunk: scratch floats per pair ~ (L/S + S + 2) * 3 * 32 * VC + 6 (L+1) + out, doubles (L+1)
+      std::vector<sxk::AdjPair> ap;
+      int64_t fo = 0, dd = 0;
+      size_t i1 = i0;
+      while (i1 < npairs) {
+        const int64_t L = t->len[pair_target[i1]];
+        const int S = std::max<int>(1, (int)std::ceil(std::sqrt((double)std::max<int64_t>(L, 1))));
+        const int64_t rowf = 3LL * 32 * VC;
+        const int64_t need_f = (L / S + 1) * rowf + (S + 1) * rowf + 6 * (L + 1) + (int64_t)out_per;
+        if (i1 > i0 && (fo + need_f) * 4 + (dd + L + 1) * 8 > budget) break;
+        sxk::AdjPair a{};
+        a.p = pair_profile[i1];
+        a.t = pair_target[i1];
+        a.S = S;
+        a.ck_off = fo;
+        a.seg_off = a.ck_off + (L / S + 1) * rowf;
+        a.sp_off = a.seg_off + (S + 1) * rowf;
+        a.out_off = a.sp_off + 6 * (L + 1);
+        a.ls_off = dd;
+        fo = a.out_off + (int64_t)out_per;
+        dd += L + 1;
+        ap.push_back(a);
+        i1++;
+      }
+      const int n = (int)ap.size();
+      e->adj_pairs.upload(ap.data(), ap.size(), s);
+      e->adj_f.alloc((size_t)fo);
+      e->adj_d.alloc((size_t)std::max<int64_t>(dd, 1));
+      e->adj_lnz.alloc((size_t)n);
+      for (const auto& a : ap)
+        CK(cudaMemsetAsync(e->adj_f.p + a.out_off, 0, sizeof(float) * out_per, s));
+      const int blocks = std::max(1, std::min((n + 3) / 4, e->num_sms * 32));
+      K.adjf[vb]<<<blocks, 128, 0, s>>>(e->adj_pairs.p, n, p->d_prof.p, p->d_vfb.p, t->d_res.p, t->d_off.p,
+                                        t->d_len.p, t->d_xsc.p, e->adj_f.p, e->adj_d.p, e->adj_lnz.p);
+      K.adjb[vb]<<<blocks, 128, 0, s>>>(e->adj_pairs.p, n, p->d_prof.p, p->d_vfb.p, t->d_res.p, t->d_off.p,
+                                        t->d_len.p, t->d_xsc.p, e->adj_f.p, e->adj_d.p, e->adj_lnz.p, e->adj_f.p);
+      CK(cudaGetLastError());
+      host_out.resize((size_t)fo);
+      CK(cudaMemcpyAsync(host_out.data(), e->adj_f.p, sizeof(float) * (size_t)fo, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(lnz + i0, e->adj_lnz.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      for (int q = 0; q < n; q++) {
+        const float* src = host_out.data() + ap[q].out_off;
+        const size_t i = i0 + (size_t)q;
+        memcpy(d_msc + i * 25 * W, src, sizeof(float) * 25 * W);
+        memcpy(d_isc + i * 25 * W, src + 25 * W, sizeof(float) * 25 * W);
+        memcpy(d_trans + i * 8 * W, src + 50 * W, sizeof(float) * 8 * W);
+      }
+      i0 = i1;
+    }
+  } catch (const CudaError& ce) {
+    return fail(ce.code, ce.msg);
+  }
+  return SX_OK;
 }
 
 }  // extern "C"

@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="shrink profile/target counts (testing only)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--plain", action="store_true", help="also time the plain one-pair-per-block kernels")
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain one-pair-per-block kernels")
     return ap.parse_args()
 
 
@@ -257,6 +257,32 @@ def main():
         torch.cuda.synchronize()
         e2e_times.append((time.perf_counter() - t) * 1e3)
         d2h = len(hits2) * 48 + len(doms2) * 56
+    # ---- the plain one-pair-per-block kernels on the same inputs ----
+    plain = None
+    if not args.no_plain:
+        peng = sxhmm.Engine(device=local, plain=True)
+        pps = peng.load_text(text, source="pfam_scale")
+        pts = peng.targets_digital(seq, offs, lens)
+        phits, _ = peng.search(pps, pts, cfg)  # warm-up
+        ptimes = []
+        for _ in range(max(1, min(args.steps, 2))):
+            flush_l2(torch, l2)
+            torch.cuda.synchronize()
+            ev0.record()
+            phits, _ = peng.search(pps, pts, cfg)
+            ev1.record()
+            torch.cuda.synchronize()
+            ptimes.append(ev0.elapsed_time(ev1))
+        pst = peng.stats()
+        plain = {"value": cells / (max(ptimes) / 1e3) / 1e9, "ms_per_step": max(ptimes), "hits": len(phits),
+                 "stage_ms": {k: round(v, 3) for k, v in zip(["msv", "bias", "viterbi", "forward", "rows",
+                                                               "host_domains", "total"], pst["ms"])},
+                 "what": "one 128-thread CTA per pair, row split across threads, shared-memory exchange + "
+                         "__syncthreads per row, block max-reduction, Viterbi D chain by one thread; same "
+                         "Forward/Backward/host stages"}
+        pps.close()
+        pts.close()
+        peng.close()
     ms_step = max(times) if times else float("nan")
     e2e_ms = max(e2e_times)
     if dist is not None:
@@ -293,6 +319,9 @@ def main():
             "stage_pairs_in": dict(zip(["msv", "bias", "viterbi", "forward", "rows", "host_domains"], stage_pairs or [])),
             "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches), "clocks": clocks}
+    if plain is not None:
+        line["plain"] = plain
+        line["batched_over_plain"] = plain["ms_per_step"] / ms_step
     if rank == 0 and not args.no_cpu_baseline and ws == 1:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline(text, seq, offs, lens, args.cpu_seconds).items()
                                 if k in ("value", "unit", "cores", "kind", "sample")}

@@ -34,6 +34,7 @@
 #include "internal.hpp"
 #include "kernels.cuh"
 #include "adjoint.cuh"
+#include "plain.cuh"
 
 using namespace sx;
 using sxk::BinRegion;
@@ -286,6 +287,8 @@ struct sx_profiles {
   std::vector<DevProfile> dp;
   std::vector<int> msv_shape;
   DevBuf<DevProfile> d_prof;
+  DevBuf<sxk::PlainProfile> d_pprof;  // plain one-pair-per-block layout
+  DevBuf<float> d_plain;
   DevBuf<float4> d_msv;
   DevBuf<float> d_vfb;
   DevBuf<double> d_bias;
@@ -444,7 +447,27 @@ void pack_profiles(sx_profiles* P) {
       b[53] = l1 / (l1 + 1.0);
     }
   }
+  // plain layout: 25 msc rows then mm mi md im ii dm dd bm, each M+1 long
+  std::vector<sxk::PlainProfile> pprof(np);
+  int64_t plain_total = 0;
+  for (size_t i = 0; i < np; i++) {
+    pprof[i].off = plain_total;
+    pprof[i].m = P->h[i].m;
+    pprof[i].pad = 0;
+    plain_total += 33LL * (P->h[i].m + 1);
+  }
+  std::vector<float> plain((size_t)std::max<int64_t>(plain_total, 1));
+  for (size_t i = 0; i < np; i++) {
+    const ProfileHost& h = P->h[i];
+    const size_t w = (size_t)h.m + 1;
+    float* b = plain.data() + pprof[i].off;
+    memcpy(b, h.msc.data(), sizeof(float) * 25 * w);
+    const int order[8] = {TMM, TMI, TMD, TIM, TII, TDM, TDD, TBM};
+    for (int q = 0; q < 8; q++) memcpy(b + (25 + q) * w, h.t[order[q]].data(), sizeof(float) * w);
+  }
   cudaStream_t s = P->eng->stream;
+  P->d_pprof.upload(pprof.data(), np, s);
+  P->d_plain.upload(plain.data(), plain.size(), s);
   P->d_prof.upload(P->dp.data(), np, s);
   P->d_msv.upload(msv.data(), msv.size(), s);
   P->d_vfb.upload(vfb.data(), vfb.size(), s);
@@ -794,6 +817,14 @@ void launch_stage(sx_engine* E, const sx_profiles* P, const sx_targets* T, int s
       if (!nin[b]) continue;
       const int blocks = (int)std::min<int64_t>((nin[b] + 7) / 8, (int64_t)E->num_sms * 16);
       cudaStream_t s = E->aux[lane++ % sx_engine::kAux];
+      if (si == 1 && (E->flags & SX_FLAG_PLAIN)) {
+        sxk::plain_viterbi_kernel<<<(unsigned)std::min<int64_t>(nin[b], (int64_t)E->num_sms * 64), sxk::kPlainThreads,
+                                    0, E->stream>>>(E->lists[1].p, cin, E->bins[1].p, b, E->lists[2].p, E->bins[2].p,
+                                                    cout, E->overflow.p, P->d_pprof.p, P->d_plain.p, E->thr.p,
+                                                    T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p, kSlackBits);
+        E->stats.kernel_launches++;
+        continue;
+      }
       if (si == 1)
         K.vit[b]<<<blocks, 256, 0, s>>>(E->lists[1].p, cin, E->bins[1].p, b, E->lists[2].p, E->bins[2].p, cout,
                                         E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
@@ -871,7 +902,19 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
       for (auto& v : tiles)
         v.erase(std::remove_if(v.begin(), v.end(), [&](const MsvTile& t) { return !th[t.p].exact; }), v.end());
       CK(cudaEventRecord(E->ev[0], s));
-      launch_msv(E, P, T, tiles, T->d_order.p, nullptr, nullptr, E->lists[0].p, E->bins[0].p, E->counts.p);
+      if (E->flags & SX_FLAG_PLAIN) {
+        const int64_t total = (int64_t)np * (int64_t)nt;
+        for (int64_t first = 0; first < total; first += (1LL << 30)) {
+          const int64_t n = std::min<int64_t>(total - first, 1LL << 30);
+          sxk::plain_msv_kernel<<<(unsigned)n, sxk::kPlainThreads, 0, s>>>(
+              first, (int)nt, P->d_pprof.p, P->d_plain.p, P->d_prof.p, E->thr.p, T->d_res.p, T->d_off.p,
+              T->d_len.p, T->d_tpar.p, E->lists[0].p, E->bins[0].p, E->counts.p, E->overflow.p);
+          E->stats.kernel_launches++;
+        }
+        CK(cudaGetLastError());
+      } else {
+        launch_msv(E, P, T, tiles, T->d_order.p, nullptr, nullptr, E->lists[0].p, E->bins[0].p, E->counts.p);
+      }
       CK(cudaEventRecord(E->ev[1], s));
       std::vector<unsigned> cnt(4 * kNumVbins);
       for (int si = 0; si < 3; si++) {

@@ -190,3 +190,16 @@ def test_search_synthetic_multiprofile(engine):
     _cmp(engine, w.hmm_text(), seqs, filters=True)
     st = engine.stats()
     assert st["pairs_in"][0] == len(w.profiles) * len(seqs)
+
+
+def test_plain_engine_same_hits():
+    """The plain one-pair-per-block kernels (SX_FLAG_PLAIN) give the same hits."""
+    w = small_config(1, 0.01)
+    seqs = [(w.target_ids[i], "".join("ACDEFGHIKLMNPQRSTVWY"[x] for x in s)) for i, s in enumerate(w.targets)]
+    plain = sxhmm.Engine(plain=True)
+    try:
+        a = _hits_oracle(w.hmm_text(), seqs, O.make_cfg())
+        b = _hits_gpu(plain, w.hmm_text(), seqs, {})
+        _assert_same_hits(a, b)
+    finally:
+        plain.close()

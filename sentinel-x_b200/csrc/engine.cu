@@ -104,6 +104,14 @@ constexpr MsvShape kMsvShapes[] = {
     {32, 8}, {32, 16}, {32, 24}, {32, 32}, {32, 40}, {32, 48}, {32, 56}, {32, 64}};
 constexpr int kNumMsvShapes = sizeof(kMsvShapes) / sizeof(kMsvShapes[0]);
 constexpr int kMaxM = 2048;
+// Viterbi lane-group shapes (G lanes per pair, C columns per lane).
+constexpr MsvShape kVitShapes[] = {{1, 8},  {2, 8},   {4, 8},   {8, 8},   {16, 8},  {32, 8},  {1, 16},
+                                   {2, 16}, {4, 16},  {8, 16},  {16, 16}, {32, 16}, {4, 24},  {8, 24},
+                                   {16, 24}, {32, 24}, {32, 32}, {32, 48}, {32, 64}};
+constexpr int kNumVitShapes = sizeof(kVitShapes) / sizeof(kVitShapes[0]);
+constexpr int kMaxBins = 32;  // survivor lists per stage (vbins or Viterbi shapes)
+static_assert(kNumVitShapes <= kMaxBins, "too many Viterbi shapes");
+
 // Warp-chunked column counts (columns per lane, 32 lanes per pair).
 constexpr int kVcBins[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64};
 constexpr int kNumVbins = sizeof(kVcBins) / sizeof(kVcBins[0]);
@@ -114,6 +122,9 @@ typedef void (*MsvFn)(const MsvTile*, const DevProfile*, const Thresholds*, cons
 typedef void (*VitFn)(const PairRec*, const unsigned*, const BinRegion*, int, PairRec*, const BinRegion*, unsigned*,
                       unsigned*, const DevProfile*, const Thresholds*, const float*, const uint8_t*, const int64_t*,
                       const int32_t*, const float4*, float, float*);
+typedef void (*VitGFn)(const PairRec*, const unsigned*, const BinRegion*, int, PairRec*, const BinRegion*, unsigned*,
+                       unsigned*, const DevProfile*, const Thresholds*, const float4*, const uint8_t*, const int64_t*,
+                       const int32_t*, const float4*, float, float*);
 typedef void (*FwdFn)(const PairRec*, const unsigned*, const BinRegion*, int, PairRec*, const BinRegion*, unsigned*,
                       unsigned*, const DevProfile*, const Thresholds*, const float*, const uint8_t*, const int64_t*,
                       const int32_t*, const float4*, float, float*, const int64_t*);
@@ -134,6 +145,17 @@ struct MsvTable {
 template <>
 struct MsvTable<kNumMsvShapes> {
   static void fill(MsvFn*) {}
+};
+template <int I>
+struct VitGTable {
+  static void fill(VitGFn* t) {
+    t[I] = sxk::viterbi_g_kernel<kVitShapes[I].g, kVitShapes[I].c>;
+    VitGTable<I + 1>::fill(t);
+  }
+};
+template <>
+struct VitGTable<kNumVitShapes> {
+  static void fill(VitGFn*) {}
 };
 template <int I>
 struct VbinTable {
@@ -158,8 +180,10 @@ struct KernelTables {
   BwdFn bwd[kNumVbins];
   AdjFFn adjf[kNumVbins];
   AdjBFn adjb[kNumVbins];
+  VitGFn vitg[kNumVitShapes];
   KernelTables() {
     MsvTable<0>::fill(msv);
+    VitGTable<0>::fill(vitg);
     VbinTable<0>::fill(vit, fwd, bwd, adjf, adjb);
   }
 };
@@ -181,6 +205,25 @@ int choose_msv_shape(int m) {
     if (g * c < m) continue;
     const double instr = 2.75 * c + 44.0 + 2.0 * std::log2((double)g);
     const double cost = instr / ((32.0 / g) * m);
+    if (cost < best_cost * 0.999) {
+      best_cost = cost;
+      best = s;
+    }
+  }
+  return best;
+}
+// Viterbi shape: per row a lane does ~19 instructions per column (16 lane-ops
+// plus 9 loads per 4 columns) and ~50 of overhead; lanes per pair cost
+// lazy-F carry rounds and butterfly steps; C >= 24 halves occupancy.
+int choose_vit_shape(int m) {
+  int best = -1;
+  double best_cost = 1e30;
+  for (int s = 0; s < kNumVitShapes; s++) {
+    const int g = kVitShapes[s].g, c = kVitShapes[s].c;
+    if (g * c < m) continue;
+    const double per_row = 19.0 * c + 50.0 + 12.0 * std::log2((double)g);
+    const double occ = c <= 16 ? 1.0 : (c <= 24 ? 0.7 : 0.5);
+    const double cost = per_row * g / (32.0 * m) / occ;
     if (cost < best_cost * 0.999) {
       best_cost = cost;
       best = s;
@@ -290,6 +333,7 @@ struct sx_profiles {
   DevBuf<sxk::PlainProfile> d_pprof;  // plain one-pair-per-block layout
   DevBuf<float> d_plain;
   DevBuf<float4> d_msv;
+  DevBuf<float4> d_vit;  // Viterbi lane-group images
   DevBuf<float> d_vfb;
   DevBuf<double> d_bias;
 };
@@ -335,7 +379,7 @@ void pack_profiles(sx_profiles* P) {
   const size_t np = P->h.size();
   P->dp.resize(np);
   P->msv_shape.resize(np);
-  int64_t msv_total = 0, vfb_total = 0;
+  int64_t msv_total = 0, vfb_total = 0, vit_total = 0;
   for (size_t i = 0; i < np; i++) {
     const ProfileHost& h = P->h[i];
     DevProfile& d = P->dp[i];
@@ -356,8 +400,13 @@ void pack_profiles(sx_profiles* P) {
     d.vfb_off = vfb_total;
     vfb_total += (int64_t)sxk::kImgRows * 32 * d.vc;
     d.msv_tbm = h.msv_tbm;
+    d.vshape = choose_vit_shape(h.m);
+    if (d.vshape < 0) throw CudaError{SX_EINVAL, "profile '" + h.name + "' too long for the Viterbi shapes"};
+    d.vit_off = vit_total;
+    vit_total += 33LL * (kVitShapes[d.vshape].c / 4) * kVitShapes[d.vshape].g;
   }
   std::vector<float4> msv((size_t)msv_total);
+  std::vector<float4> vit((size_t)std::max<int64_t>(vit_total, 1));
   std::vector<float> vfb((size_t)vfb_total);
   std::vector<double> bias(np * 54);
   for (size_t i = 0; i < np; i++) {
@@ -379,6 +428,33 @@ void pack_profiles(sx_profiles* P) {
             }
             base[((size_t)x * NC4 + c4) * G + j] = make_float4(v[0], v[1], v[2], v[3]);
           }
+    }
+    // Viterbi image: rows 0..24 log-odds, 25..32 transitions (mm im dm at k-1, bm mi ii at k,
+    // md dd at k-1), lane-major float4 chunks as for MSV
+    {
+      const int G = kVitShapes[d.vshape].g, C = kVitShapes[d.vshape].c, NC4 = C / 4;
+      float4* base = vit.data() + d.vit_off;
+      auto row = [&](int r, const std::function<float(int)>& f, float pad) {
+        for (int j = 0; j < G; j++)
+          for (int c4 = 0; c4 < NC4; c4++) {
+            float v[4];
+            for (int e = 0; e < 4; e++) {
+              const int k = j * C + c4 * 4 + e + 1;
+              v[e] = k <= m ? f(k) : pad;
+            }
+            base[((size_t)r * NC4 + c4) * G + j] = make_float4(v[0], v[1], v[2], v[3]);
+          }
+      };
+      for (int x = 0; x < 25; x++) row(x, [&](int k) { return h.msc_row(x)[k]; }, kNegInf);
+      const auto& t = h.t;
+      row(25, [&](int k) { return t[TMM][k - 1]; }, kNegInf);
+      row(26, [&](int k) { return t[TIM][k - 1]; }, kNegInf);
+      row(27, [&](int k) { return t[TDM][k - 1]; }, kNegInf);
+      row(28, [&](int k) { return t[TBM][k]; }, kNegInf);
+      row(29, [&](int k) { return t[TMI][k]; }, kNegInf);
+      row(30, [&](int k) { return t[TII][k]; }, kNegInf);
+      row(31, [&](int k) { return t[TMD][k - 1]; }, kNegInf);
+      row(32, [&](int k) { return t[TDD][k - 1]; }, kNegInf);
     }
     // warp-chunked image: row r, lane l, column c (k = l*vc + c + 1) at (r*vc + c)*32 + l
     {
@@ -470,6 +546,7 @@ void pack_profiles(sx_profiles* P) {
   P->d_plain.upload(plain.data(), plain.size(), s);
   P->d_prof.upload(P->dp.data(), np, s);
   P->d_msv.upload(msv.data(), msv.size(), s);
+  P->d_vit.upload(vit.data(), vit.size(), s);
   P->d_vfb.upload(vfb.data(), vfb.size(), s);
   P->d_bias.upload(bias.data(), bias.size(), s);
   CK(cudaStreamSynchronize(s));
@@ -551,10 +628,10 @@ struct StageLists {
 
 StageLists make_regions(const std::vector<double>& want) {
   StageLists s;
-  s.reg.resize(kNumVbins);
+  s.reg.resize(kMaxBins);
   int64_t off = 0;
-  for (int b = 0; b < kNumVbins; b++) {
-    const uint32_t cap = (uint32_t)std::min<double>(std::max(want[b], 0.0), 4.0e9);
+  for (int b = 0; b < kMaxBins; b++) {
+    const uint32_t cap = b < (int)want.size() ? (uint32_t)std::min<double>(std::max(want[b], 0.0), 4.0e9) : 0u;
     s.reg[b].off = off;
     s.reg[b].cap = cap;
     s.reg[b].pad = 0;
@@ -616,8 +693,8 @@ void rows_pass(sx_engine* E, const sx_profiles* P, const sx_targets* T, const st
     E->lists[3].upload(recs.data(), recs.size(), s);
     E->row_off.upload(roff.data(), roff.size(), s);
     E->bins[3].upload(reg.data(), reg.size(), s);
-    E->counts.alloc(4 * kNumVbins);
-    CK(cudaMemcpyAsync(E->counts.p + 3 * kNumVbins, cnt.data(), sizeof(unsigned) * kNumVbins, cudaMemcpyHostToDevice, s));
+    E->counts.alloc(4 * kMaxBins);
+    CK(cudaMemcpyAsync(E->counts.p + 3 * kMaxBins, cnt.data(), sizeof(unsigned) * kNumVbins, cudaMemcpyHostToDevice, s));
     E->rows_f.alloc((size_t)ro);
     E->rows_b.alloc((size_t)ro);
     // rows the kernels never touch are zero
@@ -628,10 +705,10 @@ void rows_pass(sx_engine* E, const sx_profiles* P, const sx_targets* T, const st
       if (!cnt[b]) continue;
       const int blocks = (int)std::min<int64_t>((cnt[b] + 7) / 8, (int64_t)E->num_sms * 16);
       cudaStream_t sa = E->aux[(2 * b) % sx_engine::kAux], sb = E->aux[(2 * b + 1) % sx_engine::kAux];
-      K.fwd[b]<<<blocks, 256, 0, sa>>>(E->lists[3].p, E->counts.p + 3 * kNumVbins, E->bins[3].p, b, nullptr, nullptr,
+      K.fwd[b]<<<blocks, 256, 0, sa>>>(E->lists[3].p, E->counts.p + 3 * kMaxBins, E->bins[3].p, b, nullptr, nullptr,
                                        nullptr, E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p,
                                        T->d_off.p, T->d_len.p, T->d_xsc.p, 0.f, E->rows_f.p, E->row_off.p);
-      K.bwd[b]<<<blocks, 256, 0, sb>>>(E->lists[3].p, E->counts.p + 3 * kNumVbins, E->bins[3].p, b, P->d_prof.p,
+      K.bwd[b]<<<blocks, 256, 0, sb>>>(E->lists[3].p, E->counts.p + 3 * kMaxBins, E->bins[3].p, b, P->d_prof.p,
                                        P->d_vfb.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p, E->rows_b.p,
                                        E->row_off.p);
       E->stats.kernel_launches += 2;
@@ -784,7 +861,9 @@ void launch_msv(sx_engine* E, const sx_profiles* P, const sx_targets* T, const s
   for (int s : order) {
     const size_t nt = start[s + 1] - start[s];
     const int g = kMsvShapes[s].g, c = kMsvShapes[s].c;
-    const size_t smem = 25ull * (c / 4) * g * sizeof(float4);
+    const int ncopy = g < 8 ? 8 / g : 1;
+    const size_t rowp = ((size_t)(c / 4) * g + 7) & ~(size_t)7;
+    const size_t smem = (size_t)ncopy * (25 * rowp + 8 + g) * sizeof(float4);
     CK(cudaFuncSetAttribute((const void*)K.msv[s], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     K.msv[s]<<<(unsigned)nt, 256, smem, E->aux[lane++ % sx_engine::kAux]>>>(
         E->tiles.p + start[s], P->d_prof.p, E->thr.p, P->d_msv.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_tpar.p,
@@ -799,8 +878,8 @@ void launch_msv(sx_engine* E, const sx_profiles* P, const sx_targets* T, const s
 void launch_stage(sx_engine* E, const sx_profiles* P, const sx_targets* T, int si, const std::vector<unsigned>& nin) {
   const auto& K = kernels();
   cudaStream_t s = E->stream;
-  unsigned* cin = E->counts.p + si * kNumVbins;
-  unsigned* cout = E->counts.p + (si + 1) * kNumVbins;
+  unsigned* cin = E->counts.p + si * kMaxBins;
+  unsigned* cout = E->counts.p + (si + 1) * kMaxBins;
   if (si == 0) {
     unsigned mx = 0;
     for (int b = 0; b < kNumVbins; b++) mx = std::max(mx, nin[b]);
@@ -808,12 +887,13 @@ void launch_stage(sx_engine* E, const sx_profiles* P, const sx_targets* T, int s
     dim3 grid((unsigned)std::min<int64_t>((mx + 255) / 256, (int64_t)E->num_sms * 8), kNumVbins);
     sxk::bias_kernel<<<grid, 256, 0, s>>>(E->lists[0].p, cin, E->bins[0].p, E->lists[1].p, E->bins[1].p, cout,
                                           E->overflow.p, P->d_bias.p, E->thr.p, T->d_res.p, T->d_off.p, T->d_len.p,
-                                          kSlackBits, nullptr);
+                                          kSlackBits, nullptr, P->d_prof.p);
     E->stats.kernel_launches++;
   } else {
     fork_aux(E);
     int lane = 0;
-    for (int b = 0; b < kNumVbins; b++) {
+    const int nb = si == 1 ? kNumVitShapes : kNumVbins;
+    for (int b = 0; b < nb; b++) {
       if (!nin[b]) continue;
       const int blocks = (int)std::min<int64_t>((nin[b] + 7) / 8, (int64_t)E->num_sms * 16);
       cudaStream_t s = E->aux[lane++ % sx_engine::kAux];
@@ -821,15 +901,18 @@ void launch_stage(sx_engine* E, const sx_profiles* P, const sx_targets* T, int s
         sxk::plain_viterbi_kernel<<<(unsigned)std::min<int64_t>(nin[b], (int64_t)E->num_sms * 64), sxk::kPlainThreads,
                                     0, E->stream>>>(E->lists[1].p, cin, E->bins[1].p, b, E->lists[2].p, E->bins[2].p,
                                                     cout, E->overflow.p, P->d_pprof.p, P->d_plain.p, E->thr.p,
-                                                    T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p, kSlackBits);
+                                                    T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p, kSlackBits,
+                                                    P->d_prof.p);
         E->stats.kernel_launches++;
         continue;
       }
-      if (si == 1)
-        K.vit[b]<<<blocks, 256, 0, s>>>(E->lists[1].p, cin, E->bins[1].p, b, E->lists[2].p, E->bins[2].p, cout,
-                                        E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
-                                        T->d_len.p, T->d_xsc.p, kSlackBits, nullptr);
-      else
+      if (si == 1) {
+        const int g = kVitShapes[b].g;
+        const int vblocks = (int)std::min<int64_t>(((int64_t)nin[b] * g + 255) / 256, (int64_t)E->num_sms * 16);
+        K.vitg[b]<<<vblocks, 256, 0, s>>>(E->lists[1].p, cin, E->bins[1].p, b, E->lists[2].p, E->bins[2].p, cout,
+                                          E->overflow.p, P->d_prof.p, E->thr.p, P->d_vit.p, T->d_res.p, T->d_off.p,
+                                          T->d_len.p, T->d_xsc.p, kSlackBits, nullptr);
+      } else
         K.fwd[b]<<<blocks, 256, 0, s>>>(E->lists[2].p, cin, E->bins[2].p, b, E->lists[3].p, E->bins[3].p, cout,
                                         E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
                                         T->d_len.p, T->d_xsc.p, kSlackBits, nullptr, nullptr);
@@ -862,7 +945,7 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
   std::vector<Thresholds> th = make_thresholds(P->h, o);
   E->thr.upload(th.data(), th.size(), s);
   E->overflow.alloc(1);
-  E->counts.alloc(4 * kNumVbins);
+  E->counts.alloc(4 * kMaxBins);
   std::vector<FinalPair> finals;
   auto t_start = std::chrono::steady_clock::now();
 
@@ -875,27 +958,29 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
 
   if (any_filtered && nt > 0) {
     // capacity per vbin from the number of pairs it holds
-    std::vector<double> pairs_in_bin(kNumVbins, 0.0);
+    std::vector<double> pairs_in_bin(kMaxBins, 0.0), pairs_in_vs(kMaxBins, 0.0);
     double cells_total = 0;
     for (size_t pi = 0; pi < np; pi++)
       if (th[pi].exact) {
         pairs_in_bin[P->dp[pi].vbin] += (double)nt;
+        pairs_in_vs[P->dp[pi].vshape] += (double)nt;
         cells_total += (double)P->h[pi].m * T->residues;
       }
     double scale = 1.0;
     for (int attempt = 0; attempt < 4; attempt++) {
-      std::vector<double> w1(kNumVbins), w3(kNumVbins);
-      for (int b = 0; b < kNumVbins; b++) {
+      std::vector<double> w1(kMaxBins), w1v(kMaxBins), w3(kMaxBins);
+      for (int b = 0; b < kMaxBins; b++) {
         w1[b] = pairs_in_bin[b] > 0 ? std::min(pairs_in_bin[b], scale * (0.06 * pairs_in_bin[b] + 8192)) : 0;
+        w1v[b] = pairs_in_vs[b] > 0 ? std::min(pairs_in_vs[b], scale * (0.06 * pairs_in_vs[b] + 8192)) : 0;
         w3[b] = pairs_in_bin[b] > 0 ? std::min(pairs_in_bin[b], scale * (0.01 * pairs_in_bin[b] + 4096)) : 0;
       }
-      StageLists L0 = make_regions(w1), L1 = make_regions(w1), L2 = make_regions(w3), L3 = make_regions(w3);
+      StageLists L0 = make_regions(w1), L1 = make_regions(w1v), L2 = make_regions(w3), L3 = make_regions(w3);
       StageLists* Ls[4] = {&L0, &L1, &L2, &L3};
       for (int q = 0; q < 4; q++) {
         E->lists[q].alloc((size_t)Ls[q]->total);
-        E->bins[q].upload(Ls[q]->reg.data(), kNumVbins, s);
+        E->bins[q].upload(Ls[q]->reg.data(), kMaxBins, s);
       }
-      CK(cudaMemsetAsync(E->counts.p, 0, sizeof(unsigned) * 4 * kNumVbins, s));
+      CK(cudaMemsetAsync(E->counts.p, 0, sizeof(unsigned) * 4 * kMaxBins, s));
       CK(cudaMemsetAsync(E->overflow.p, 0, sizeof(unsigned), s));
       // stage 0: MSV over all pairs of filtered profiles
       auto tiles = make_all_pairs_tiles(E, P, T);
@@ -916,18 +1001,18 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
         launch_msv(E, P, T, tiles, T->d_order.p, nullptr, nullptr, E->lists[0].p, E->bins[0].p, E->counts.p);
       }
       CK(cudaEventRecord(E->ev[1], s));
-      std::vector<unsigned> cnt(4 * kNumVbins);
+      std::vector<unsigned> cnt(4 * kMaxBins);
       for (int si = 0; si < 3; si++) {
-        CK(cudaMemcpyAsync(cnt.data(), E->counts.p, sizeof(unsigned) * 4 * kNumVbins, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(cnt.data(), E->counts.p, sizeof(unsigned) * 4 * kMaxBins, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
-        std::vector<unsigned> nin(kNumVbins);
-        for (int b = 0; b < kNumVbins; b++) nin[b] = std::min(cnt[si * kNumVbins + b], Ls[si]->reg[b].cap);
+        std::vector<unsigned> nin(kMaxBins);
+        for (int b = 0; b < kMaxBins; b++) nin[b] = std::min(cnt[si * kMaxBins + b], Ls[si]->reg[b].cap);
         CK(cudaEventRecord(E->ev[2 + si], s));
         launch_stage(E, P, T, si, nin);
       }
       CK(cudaEventRecord(E->ev[5], s));
       unsigned ovf = 0;
-      CK(cudaMemcpyAsync(cnt.data(), E->counts.p, sizeof(unsigned) * 4 * kNumVbins, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(cnt.data(), E->counts.p, sizeof(unsigned) * 4 * kMaxBins, cudaMemcpyDeviceToHost, s));
       CK(cudaMemcpyAsync(&ovf, E->overflow.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
       if (ovf) {  // a survivor list was too small: grow and rerun
@@ -936,12 +1021,12 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
       }
       // stats
       double pairs_all = 0;
-      for (int b = 0; b < kNumVbins; b++) pairs_all += pairs_in_bin[b];
+      for (int b = 0; b < kMaxBins; b++) pairs_all += pairs_in_bin[b];
       E->stats.pairs_in[0] = (int64_t)pairs_all;
       E->stats.cells[0] = cells_total;
       for (int si = 0; si < 4; si++) {
         int64_t c = 0;
-        for (int b = 0; b < kNumVbins; b++) c += cnt[si * kNumVbins + b];
+        for (int b = 0; b < kMaxBins; b++) c += cnt[si * kMaxBins + b];
         E->stats.pairs_out[si] = c;
         if (si < 3) E->stats.pairs_in[si + 1] = c;
       }
@@ -952,7 +1037,7 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
       // gather stage-3 survivors
       std::vector<PairRec> surv;
       for (int b = 0; b < kNumVbins; b++) {
-        const unsigned n = std::min(cnt[3 * kNumVbins + b], L3.reg[b].cap);
+        const unsigned n = std::min(cnt[3 * kMaxBins + b], L3.reg[b].cap);
         if (!n) continue;
         const size_t o0 = surv.size();
         surv.resize(o0 + n);
@@ -1277,11 +1362,11 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
     if (bias || viterbi) {
       // pair lists per vbin, every pair carries its slot
       std::vector<PairRec> recs;
-      std::vector<BinRegion> reg(kNumVbins);
-      std::vector<unsigned> cnt(kNumVbins, 0);
-      std::vector<std::vector<int32_t>> byb(kNumVbins);
-      for (size_t i = 0; i < npairs; i++) byb[p->dp[pair_profile[i]].vbin].push_back((int32_t)i);
-      for (int b = 0; b < kNumVbins; b++) {
+      std::vector<BinRegion> reg(kMaxBins);
+      std::vector<unsigned> cnt(kMaxBins, 0);
+      std::vector<std::vector<int32_t>> byb(kMaxBins);
+      for (size_t i = 0; i < npairs; i++) byb[p->dp[pair_profile[i]].vshape].push_back((int32_t)i);
+      for (int b = 0; b < kMaxBins; b++) {
         reg[b].off = (int64_t)recs.size();
         reg[b].cap = (uint32_t)byb[b].size();
         reg[b].pad = 0;
@@ -1290,26 +1375,28 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
       }
       e->lists[0].upload(recs.data(), recs.size(), s);
       e->bins[0].upload(reg.data(), reg.size(), s);
-      e->counts.alloc(4 * kNumVbins);
-      CK(cudaMemcpyAsync(e->counts.p, cnt.data(), sizeof(unsigned) * kNumVbins, cudaMemcpyHostToDevice, s));
+      e->counts.alloc(4 * kMaxBins);
+      CK(cudaMemcpyAsync(e->counts.p, cnt.data(), sizeof(unsigned) * kMaxBins, cudaMemcpyHostToDevice, s));
       const auto& K = kernels();
       if (bias) {
         unsigned mx = *std::max_element(cnt.begin(), cnt.end());
-        dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>((mx + 255) / 256, (int64_t)e->num_sms * 8)), kNumVbins);
+        dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>((mx + 255) / 256, (int64_t)e->num_sms * 8)),
+                  kNumVitShapes);
         sxk::bias_kernel<<<grid, 256, 0, s>>>(e->lists[0].p, e->counts.p, e->bins[0].p, nullptr, nullptr, nullptr,
                                               e->overflow.p, p->d_bias.p, e->thr.p, t->d_res.p, t->d_off.p, t->d_len.p,
-                                              0.f, e->scores.p);
+                                              0.f, e->scores.p, p->d_prof.p);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(bias, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
       }
       if (viterbi) {
-        for (int b = 0; b < kNumVbins; b++) {
+        for (int b = 0; b < kNumVitShapes; b++) {
           if (!cnt[b]) continue;
-          const int blocks = (int)std::min<int64_t>((cnt[b] + 7) / 8, (int64_t)e->num_sms * 16);
-          K.vit[b]<<<blocks, 256, 0, s>>>(e->lists[0].p, e->counts.p, e->bins[0].p, b, nullptr, nullptr, nullptr,
-                                          e->overflow.p, p->d_prof.p, e->thr.p, p->d_vfb.p, t->d_res.p, t->d_off.p,
-                                          t->d_len.p, t->d_xsc.p, 0.f, e->scores.p);
+          const int g = kVitShapes[b].g;
+          const int blocks = (int)std::min<int64_t>(((int64_t)cnt[b] * g + 255) / 256, (int64_t)e->num_sms * 16);
+          K.vitg[b]<<<blocks, 256, 0, s>>>(e->lists[0].p, e->counts.p, e->bins[0].p, b, nullptr, nullptr, nullptr,
+                                           e->overflow.p, p->d_prof.p, e->thr.p, p->d_vit.p, t->d_res.p, t->d_off.p,
+                                           t->d_len.p, t->d_xsc.p, 0.f, e->scores.p);
         }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(viterbi, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));

@@ -20,7 +20,7 @@ constexpr float kLn2 = 0.693147182464599609375f;
 constexpr unsigned kFull = 0xffffffffu;
 
 // ---- device records ------------------------------------------------------
-struct DevProfile {  // 48 bytes
+struct DevProfile {  // 56 bytes
   int32_t m;
   int32_t vc;        // columns per lane in the warp-chunked layout (32 lanes)
   int32_t vbin;      // survivor-list bin of vc
@@ -30,7 +30,8 @@ struct DevProfile {  // 48 bytes
   int64_t msv_off;   // float4 offset of the MSV shared-memory image
   int64_t vfb_off;   // float offset of the warp-chunked image (kImgRows rows of 32*vc)
   float msv_tbm;
-  int32_t pad1;
+  int32_t vshape;    // Viterbi lane-group shape (index into the engine's shape table)
+  int64_t vit_off;   // float4 offset of the Viterbi image (33 rows, lane-major for that shape)
 };
 struct Thresholds {  // per profile, per search: pass iff statistic >= threshold (bits)
   float s1, s2, s3;
@@ -104,19 +105,32 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
   static_assert(C % 8 == 0 && (G & (G - 1)) == 0 && G <= 32, "bad MSV shape");
   constexpr int NC4 = C / 4;
   constexpr int ROW4 = NC4 * G;  // float4 per residue row
+  // A quarter-warp (8 lanes) issues one LDS.128 wavefront: with G < 8 it holds
+  // 8/G groups reading rows of different residues.  Each of those groups reads
+  // its own copy of the image, copy q shifted by q*G float4 (q*16G bytes)
+  // inside the 128-byte bank window, so their chunks never share a bank.
+  constexpr int NCOPY = G < 8 ? 8 / G : 1;
+  constexpr int ROWP = (ROW4 + 7) & ~7;            // row stride padded to 128 bytes
+  constexpr int COPY4 = 25 * ROWP + 8;             // float4 per copy, +8 keeps copies 128-byte aligned
   extern __shared__ float4 sm_rows[];
   __shared__ int s_next;
   const MsvTile tile = tiles[blockIdx.x];
   const DevProfile P = profs[tile.p];
   {
     const float4* src = msv_img + P.msv_off;
-    for (int q = threadIdx.x; q < 25 * ROW4; q += blockDim.x) sm_rows[q] = src[q];
+    for (int q = threadIdx.x; q < 25 * ROW4; q += blockDim.x) {
+      const int x = q / ROW4, e = q - x * ROW4;
+      const float4 v = src[q];
+#pragma unroll
+      for (int cp = 0; cp < NCOPY; cp++) sm_rows[cp * COPY4 + cp * G + x * ROWP + e] = v;
+    }
   }
   if (threadIdx.x == 0) s_next = tile.begin;
   __syncthreads();
 
   const int lane = threadIdx.x & 31;
   const int j = lane & (G - 1);
+  const float4* my_rows = sm_rows + ((lane >> 0) / G % NCOPY) * (COPY4 + G);
   const int gl = lane - j;
   const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << gl);
   const float tbm = P.msv_tbm;
@@ -178,7 +192,7 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
 #pragma unroll
     for (int r = 0; r < 4; r++) {
       const int x = (w >> (8 * r)) & 0xff;
-      const float4* rowp = sm_rows + x * ROW4 + j;
+      const float4* rowp = my_rows + x * ROWP + j;
       float4 rv[NC4];
 #pragma unroll
       for (int c4 = 0; c4 < NC4; c4++) rv[c4] = rowp[c4 * G];
@@ -232,7 +246,8 @@ __global__ void __launch_bounds__(256) bias_kernel(const PairRec* __restrict__ i
                                                    unsigned* __restrict__ overflow, const double* __restrict__ btab,
                                                    const Thresholds* __restrict__ thr, const uint8_t* __restrict__ res,
                                                    const int64_t* __restrict__ toff, const int32_t* __restrict__ tlen,
-                                                   float slack, float* __restrict__ score_out) {
+                                                   float slack, float* __restrict__ score_out,
+                                                   const DevProfile* __restrict__ profs) {
   const int bin = blockIdx.y;
   const unsigned n = min(in_counts[bin], in_bins[bin].cap);
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -266,7 +281,7 @@ __global__ void __launch_bounds__(256) bias_kernel(const PairRec* __restrict__ i
       score_out[r.slot] = fsc;
       continue;
     }
-    if (bits_stat(r.usc, fsc) >= thr[r.p].s1 - slack) push_pair(r, bin, out, out_bins, out_counts, overflow);
+    if (bits_stat(r.usc, fsc) >= thr[r.p].s1 - slack) push_pair(r, profs[r.p].vshape, out, out_bins, out_counts, overflow);
   }
 }
 
@@ -749,6 +764,173 @@ __global__ void __launch_bounds__(256) backward_kernel(
         orow[0] = 0.f; orow[1] = b; orow[2] = 0.f; orow[3] = 0.f; orow[4] = 0.f; orow[5] = 0.f;
       }
     }
+  }
+}
+
+}  // namespace sxk
+
+namespace sxk {
+
+// ===========================================================================
+// Viterbi filter, lane-group form (src/hmmer/dp.rs:152-189).  A warp holds
+// 32/G pairs; a group of G lanes scores one pair, lane j holding columns
+// j*C+1 .. j*C+C.  The profile's 33 score rows (25 log-odds, 8 transitions
+// shifted so column k reads its own slot) are a lane-major float4 image read
+// through L1, four columns per 16-byte load.  A row is updated in place: M and
+// I descending (each needs the old values at k and k-1), then the D chain
+// ascending with carry -inf at the lane boundary, then carries are pushed
+// across the group's lanes until nothing changes (exact, as fl(x+t) is
+// monotone in x).  All groups step rows in lock step; a group that finishes a
+// pair takes the next one, and the score is latched at its last row.
+// ===========================================================================
+template <int G, int C>
+__global__ void __launch_bounds__(256) viterbi_g_kernel(
+    const PairRec* __restrict__ in, const unsigned* __restrict__ in_counts, const BinRegion* __restrict__ in_bins,
+    int bin, PairRec* __restrict__ out, const BinRegion* __restrict__ out_bins, unsigned* __restrict__ out_counts,
+    unsigned* __restrict__ overflow, const DevProfile* __restrict__ profs, const Thresholds* __restrict__ thr,
+    const float4* __restrict__ vimg, const uint8_t* __restrict__ res, const int64_t* __restrict__ toff,
+    const int32_t* __restrict__ tlen, const float4* __restrict__ xsc, float slack, float* __restrict__ score_out) {
+  static_assert(C % 8 == 0 && (G & (G - 1)) == 0 && G <= 32, "bad Viterbi shape");
+  constexpr int NC4 = C / 4;
+  constexpr int ROW4 = NC4 * G;
+  const int lane = threadIdx.x & 31;
+  const int j = lane & (G - 1);
+  const int gl = lane - j;
+  const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << gl);
+  const unsigned n = min(in_counts[bin], in_bins[bin].cap);
+  const int64_t base = in_bins[bin].off;
+  const unsigned ngroups = (gridDim.x * blockDim.x) / G;
+  unsigned next = (blockIdx.x * blockDim.x + threadIdx.x) / G;  // this group's next list position
+
+  float mp[C], ip[C], dp[C];
+  float xn = 0.f, xb = 0.f, xj = SX_NEG_INF, xc = SX_NEG_INF, fin = SX_NEG_INF;
+  float lloop = 0.f, lmove = 0.f;
+  int M = 0, L = 0, row = 0;
+  bool active = false, done = false;
+  PairRec r{};
+  const float4* img = vimg;
+  const uint8_t* s = res;
+  for (;;) {
+    if (!done && row >= L) {  // group-uniform: finish the pair, take the next one
+      if (active && j == 0) {
+        r.vsc = fin;
+        if (score_out) score_out[r.slot] = fin;
+        else if (bits_stat(fin, r.filtersc) >= thr[r.p].s2 - slack)
+          push_pair(r, profs[r.p].vbin, out, out_bins, out_counts, overflow);
+      }
+      if (next < n) {
+        r = in[base + next];
+        next += ngroups;
+        const DevProfile P = profs[r.p];
+        img = vimg + P.vit_off;
+        M = P.m;
+        L = tlen[r.t];
+        s = res + toff[r.t];
+        const float4 xs = xsc[r.t];
+        lloop = xs.x;
+        lmove = xs.y;
+        xn = 0.f; xb = lmove; xj = SX_NEG_INF; xc = SX_NEG_INF;
+        fin = SX_NEG_INF;
+#pragma unroll
+        for (int c = 0; c < C; c++) mp[c] = ip[c] = dp[c] = SX_NEG_INF;
+        row = 0;
+        active = true;
+      } else {
+        active = false;
+        done = true;
+        L = 0;
+      }
+    }
+    if (__all_sync(kFull, done)) break;
+    const int x = (active && row < L) ? __ldg(s + row) : 24;
+    const bool ins_ok = x != 24;
+    const float4* rowx = img + x * ROW4 + j;
+    const float4* tr = img + 25 * ROW4 + j;  // transition rows: mm im dm bm mi ii md dd
+    // ---- M and I, descending (old values at c and c-1 still in place) ----
+    const float mpl0 = __shfl_up_sync(kFull, mp[C - 1], 1, G);
+    const float ipl0 = __shfl_up_sync(kFull, ip[C - 1], 1, G);
+    const float dpl0 = __shfl_up_sync(kFull, dp[C - 1], 1, G);
+    const float mpl = j ? mpl0 : SX_NEG_INF, ipl = j ? ipl0 : SX_NEG_INF, dpl = j ? dpl0 : SX_NEG_INF;
+#pragma unroll
+    for (int c4 = NC4 - 1; c4 >= 0; c4--) {
+      const float4 tmm = tr[(0 * NC4 + c4) * G], tim = tr[(1 * NC4 + c4) * G], tdm = tr[(2 * NC4 + c4) * G];
+      const float4 tbm = tr[(3 * NC4 + c4) * G], tmi = tr[(4 * NC4 + c4) * G], tii = tr[(5 * NC4 + c4) * G];
+      const float4 sc4 = rowx[c4 * G];
+#pragma unroll
+      for (int e = 3; e >= 0; e--) {
+        const int c = 4 * c4 + e;
+        const int k = j * C + c + 1;
+        auto pick = [e](const float4& v) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; };
+        const float mpv = c ? mp[c - 1] : mpl, ipv = c ? ip[c - 1] : ipl, dpv = c ? dp[c - 1] : dpl;
+        const float ni = (k < M && ins_ok) ? fmx(fadd(mp[c], pick(tmi)), fadd(ip[c], pick(tii))) : SX_NEG_INF;
+        const float sc = fmx(fmx(fadd(mpv, pick(tmm)), fadd(ipv, pick(tim))), fmx(fadd(xb, pick(tbm)), fadd(dpv, pick(tdm))));
+        mp[c] = fadd(sc, pick(sc4));
+        ip[c] = ni;
+      }
+    }
+    // ---- D chain, ascending, carry -inf at the lane boundary ----
+    const float mcl0 = __shfl_up_sync(kFull, mp[C - 1], 1, G);
+    float d = SX_NEG_INF;
+#pragma unroll
+    for (int c4 = 0; c4 < NC4; c4++) {
+      const float4 tmd = tr[(6 * NC4 + c4) * G], tdd = tr[(7 * NC4 + c4) * G];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int c = 4 * c4 + e;
+        auto pick = [e](const float4& v) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; };
+        const float mcv = c ? mp[c - 1] : (j ? mcl0 : SX_NEG_INF);
+        d = fmx(fadd(mcv, pick(tmd)), fadd(d, pick(tdd)));
+        dp[c] = d;
+      }
+    }
+    // ---- push carries across the group's lanes (at most G-1 rounds) ----
+    for (int it = 0; it < G; it++) {
+      const float cin0 = __shfl_up_sync(kFull, dp[C - 1], 1, G);
+      float cin = j ? cin0 : SX_NEG_INF;
+      bool go = true, changed = false;
+#pragma unroll
+      for (int c4 = 0; c4 < NC4; c4++) {
+        if (go) {
+          const float4 tdd = tr[(7 * NC4 + c4) * G];
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const int c = 4 * c4 + e;
+            const float t = e == 0 ? tdd.x : e == 1 ? tdd.y : e == 2 ? tdd.z : tdd.w;
+            if (go) {
+              const float cand = fadd(cin, t);
+              if (cand > dp[c]) {
+                dp[c] = cand;
+                cin = cand;
+                changed = true;
+              } else {
+                go = false;
+              }
+            }
+          }
+        }
+      }
+      if (!__any_sync(kFull, changed)) break;
+    }
+    // ---- row maximum and special states ----
+    float blk[C / 8];
+#pragma unroll
+    for (int b = 0; b < C / 8; b++) {
+      const float* mv = mp + 8 * b;
+      const float* dv = dp + 8 * b;
+      blk[b] = fmx3(fmx3(fmx3(mv[0], mv[1], mv[2]), fmx3(mv[3], mv[4], mv[5]), fmx(mv[6], mv[7])),
+                    fmx3(dv[0], dv[1], dv[2]), fmx3(fmx3(dv[3], dv[4], dv[5]), dv[6], dv[7]));
+    }
+    float xe = blk[0];
+#pragma unroll
+    for (int b = 1; b < C / 8; b++) xe = fmx(xe, blk[b]);
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1) xe = fmx(xe, __shfl_xor_sync(kFull, xe, o, G));
+    xj = fmx(fadd(xj, lloop), fadd(xe, -kLn2));
+    xc = fmx(fadd(xc, lloop), fadd(xe, -kLn2));
+    xn = fadd(xn, lloop);
+    xb = fmx(fadd(xn, lmove), fadd(xj, lmove));
+    row++;
+    if (row == L) fin = fadd(xc, lmove);
   }
 }
 

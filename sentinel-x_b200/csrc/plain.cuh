@@ -102,7 +102,8 @@ __global__ void __launch_bounds__(kPlainThreads) plain_viterbi_kernel(
     int bin, PairRec* __restrict__ out, const BinRegion* __restrict__ out_bins, unsigned* __restrict__ out_counts,
     unsigned* __restrict__ overflow, const PlainProfile* __restrict__ pprof, const float* __restrict__ pimg,
     const Thresholds* __restrict__ thr, const uint8_t* __restrict__ res, const int64_t* __restrict__ toff,
-    const int32_t* __restrict__ tlen, const float4* __restrict__ xsc, float slack) {
+    const int32_t* __restrict__ tlen, const float4* __restrict__ xsc, float slack,
+    const DevProfile* __restrict__ profs) {
   __shared__ float sm[2049], si[2049], sd[2049], mc[2049], dcur[2049];
   __shared__ float red[kPlainThreads / 32];
   const unsigned n = min(in_counts[bin], in_bins[bin].cap);
@@ -162,7 +163,8 @@ __global__ void __launch_bounds__(kPlainThreads) plain_viterbi_kernel(
     }
     if (threadIdx.x == 0) {
       r.vsc = (L > 0 && M > 0) ? fadd(xc, xs.y) : SX_NEG_INF;
-      if (bits_stat(r.vsc, r.filtersc) >= thr[r.p].s2 - slack) push_pair(r, bin, out, out_bins, out_counts, overflow);
+      if (bits_stat(r.vsc, r.filtersc) >= thr[r.p].s2 - slack)
+        push_pair(r, profs[r.p].vbin, out, out_bins, out_counts, overflow);
     }
     __syncthreads();
   }

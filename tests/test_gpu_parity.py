@@ -203,3 +203,25 @@ def test_plain_engine_same_hits():
         _assert_same_hits(a, b)
     finally:
         plain.close()
+
+
+def test_forward_error_vs_fp64_logspace(engine):
+    """FP32 odds-space Forward with per-row scaling (bit-identical to the
+    reference) against an FP64 log-space Forward: within 0.01 bits."""
+    rng = np.random.default_rng(3)
+    for cfg, scale in ((0, 0.05), (1, 0.004), (3, 1 / 16)):
+        w = small_config(cfg, scale) if cfg != 3 else __import__("sxhmm").synth.make_config(3, scale=scale)
+        text = w.hmm_text()
+        o = O.Oracle(text=text)
+        ps = engine.load_text(text)
+        lens = np.array([len(s) for s in w.targets], np.int64)
+        offs = np.zeros(len(lens), np.int64)
+        offs[1:] = np.cumsum(lens)[:-1]
+        ts = engine.targets_digital(np.concatenate(w.targets), offs, lens)
+        pairs = w.pairs or [(p, t) for p in range(len(w.profiles)) for t in range(len(w.targets))]
+        pick = rng.choice(len(pairs), size=min(60, len(pairs)), replace=False)
+        pp = np.array([pairs[q][0] for q in pick], np.int32)
+        pt = np.array([pairs[q][1] for q in pick], np.int32)
+        fwd = engine.score_pairs(ps, ts, pp, pt, stages=("forward",))["forward"]
+        err = [abs(float(f) - o.forward_f64(int(a), w.targets[b])) / np.log(2) for f, a, b in zip(fwd, pp, pt)]
+        assert max(err) < 0.01, (cfg, max(err))

@@ -222,7 +222,7 @@ int choose_vit_shape(int m) {
     const int g = kVitShapes[s].g, c = kVitShapes[s].c;
     if (g * c < m) continue;
     const double per_row = 19.0 * c + 50.0 + 12.0 * std::log2((double)g);
-    const double occ = c <= 16 ? 1.0 : (c <= 24 ? 0.7 : 0.5);
+    const double occ = c <= 16 ? 1.0 : 0.5;  // C <= 16 runs two 256-thread CTAs per SM, wider C one
     const double cost = per_row * g / (32.0 * m) / occ;
     if (cost < best_cost * 0.999) {
       best_cost = cost;

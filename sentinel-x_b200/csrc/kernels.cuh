@@ -784,7 +784,7 @@ namespace sxk {
 // pair takes the next one, and the score is latched at its last row.
 // ===========================================================================
 template <int G, int C>
-__global__ void __launch_bounds__(256) viterbi_g_kernel(
+__global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
     const PairRec* __restrict__ in, const unsigned* __restrict__ in_counts, const BinRegion* __restrict__ in_bins,
     int bin, PairRec* __restrict__ out, const BinRegion* __restrict__ out_bins, unsigned* __restrict__ out_counts,
     unsigned* __restrict__ overflow, const DevProfile* __restrict__ profs, const Thresholds* __restrict__ thr,

@@ -34,6 +34,7 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 METRIC = "Plan7 GCUPS (MSV/Vit/Fwd/Bwd), batched vs plain on 1 B200; hits bit-exact"
+STAGES = ["msv", "bias", "viterbi", "forward", "rows", "host_domains", "total", "host_tail"]
 WORKLOAD = ("pfam_scale: 1000 profiles M~LN(150,0.5)[20,1000] x 50000 targets L~LN(300,0.6)[30,3000], "
             "2% planted homologs, E<=10, F1/F2/F3 = 0.02/1e-3/1e-5")
 MSV_OPS_PER_CELL = 3  # 1 FADD + 2 FMAX per cell (src/hmmer/dp.rs:122-124)
@@ -49,6 +50,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain one-pair-per-block kernels")
+    ap.add_argument("--pipeline-blocks", type=int, default=0,
+                    help="profile blocks per search (0 = engine default by workload size)")
     return ap.parse_args()
 
 
@@ -199,7 +202,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     import sxhmm
     from sxhmm import synth
-    eng = sxhmm.Engine(device=local)
+    eng = sxhmm.Engine(device=local, pipeline_blocks=args.pipeline_blocks)
     t0 = time.time()
     text, seq, offs, lens, nt = workload(args.scale, rank, scorer=synth.engine_scorer(eng))
     gen_s = time.time() - t0
@@ -220,7 +223,7 @@ def main():
         eng.search(ps, ts, cfg)
     sampler = ClockSampler(local)
     sampler.start()
-    times, msv_ms, msv_cells, launches, nhits = [], [], [], 0, 0
+    times, launches, nhits = [], 0, 0
     stage_ms = np.zeros(8)
     stage_pairs = None
     for _ in range(args.steps):
@@ -234,15 +237,13 @@ def main():
         barrier()
         times.append(ev0.elapsed_time(ev1))
         st = eng.stats()
-        msv_ms.append(st["ms"][0])
-        msv_cells.append(st["cells"][0])
         stage_ms += np.array(st["ms"])
         launches = st["kernel_launches"]
         stage_pairs = st["pairs_in"][:6]
         nhits = len(hits)
     clocks = sampler.stop()
     # ---- end-to-end steps through the C ABI with host buffers ----
-    e2e_times = []
+    e2e_times, e2e_upload, e2e_stage, e2e_parts = [], [], [], []
     h2d = int(seq.nbytes + offs.nbytes + lens.nbytes)
     d2h = 0
     pinned = torch.from_numpy(seq).pin_memory().numpy()
@@ -252,15 +253,44 @@ def main():
         torch.cuda.synchronize()
         t = time.perf_counter()
         ts2 = eng.targets_digital(pinned, offs, lens)
+        t_up = time.perf_counter()
         hits2, doms2 = eng.search(ps, ts2, cfg)
+        t_se = time.perf_counter()
+        torch.cuda.synchronize()
+        t_sy = time.perf_counter()
         ts2.close()
+        t_cl = time.perf_counter()
         torch.cuda.synchronize()
         e2e_times.append((time.perf_counter() - t) * 1e3)
+        e2e_upload.append((t_up - t) * 1e3)
+        e2e_parts.append([round((t_se - t_up) * 1e3, 1), round((t_sy - t_se) * 1e3, 1), round((t_cl - t_sy) * 1e3, 1)])
+        e2e_stage.append({k: round(v, 1) for k, v in zip(STAGES, eng.stats()["ms"])})
         d2h = len(hits2) * 48 + len(doms2) * 56
+    # ---- MSV kernel alone: a single-block search, where MSV does not share the
+    # GPU with later stages of another block, gives the kernel's own event time ----
+    reng = sxhmm.Engine(device=local, pipeline_blocks=1)
+    rps = reng.load_text(text, source="pfam_scale")
+    rts = reng.targets_digital(seq, offs, lens)
+    reng.search(rps, rts, cfg)  # warm-up
+    msv_ms, msv_cells, single_ms = [], [], []
+    for _ in range(2):
+        flush_l2(torch, l2)
+        torch.cuda.synchronize()
+        ev0.record()
+        reng.search(rps, rts, cfg)
+        ev1.record()
+        torch.cuda.synchronize()
+        single_ms.append(ev0.elapsed_time(ev1))
+        rst = reng.stats()
+        msv_ms.append(rst["ms"][0])
+        msv_cells.append(rst["cells"][0])
+    rps.close()
+    rts.close()
+    reng.close()
     # ---- the plain one-pair-per-block kernels on the same inputs ----
     plain = None
     if not args.no_plain:
-        peng = sxhmm.Engine(device=local, plain=True)
+        peng = sxhmm.Engine(device=local, plain=True, pipeline_blocks=args.pipeline_blocks)
         pps = peng.load_text(text, source="pfam_scale")
         pts = peng.targets_digital(seq, offs, lens)
         phits, _ = peng.search(pps, pts, cfg)  # warm-up
@@ -275,8 +305,7 @@ def main():
             ptimes.append(ev0.elapsed_time(ev1))
         pst = peng.stats()
         plain = {"value": cells / (max(ptimes) / 1e3) / 1e9, "ms_per_step": max(ptimes), "hits": len(phits),
-                 "stage_ms": {k: round(v, 3) for k, v in zip(["msv", "bias", "viterbi", "forward", "rows",
-                                                               "host_domains", "total"], pst["ms"])},
+                 "stage_ms": {k: round(v, 3) for k, v in zip(STAGES, pst["ms"])},
                  "what": "one 128-thread CTA per pair, row split across threads, shared-memory exchange + "
                          "__syncthreads per row, block max-reduction, Viterbi D chain by one thread; same "
                          "Forward/Backward/host stages"}
@@ -313,11 +342,18 @@ def main():
                        "generation_s": round(gen_s, 1), "hits": nhits, "hmm_sha1": sha1(text)},
             "roofline": {"bound": "alu", "kernel": "msv_kernel", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
-                         "peak_note": "148 SMs x 128 FP32 lanes x median sampled SM clock (lane-ops/s)"},
-            "stage_ms": {k: round(v / max(1, args.steps), 3) for k, v in zip(
-                ["msv", "bias", "viterbi", "forward", "rows", "host_domains", "total"], stage_ms)},
+                         "peak_note": "148 SMs x 128 FP32 lanes x median sampled SM clock (lane-ops/s)",
+                         "kernel_ms": round(msv_t * 1e3, 3),
+                         "measured_in": "single-block search (pipeline_blocks=1): MSV launches alone on the GPU, "
+                                        "CUDA events around them",
+                         "single_block_ms_per_step": round(max(single_ms), 3)},
+            "stage_ms": {k: round(v / max(1, args.steps), 3) for k, v in zip(STAGES, stage_ms)},
             "stage_pairs_in": dict(zip(["msv", "bias", "viterbi", "forward", "rows", "host_domains"], stage_pairs or [])),
-            "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps_ms": [round(x, 1) for x in e2e_times],
+                    "target_upload_ms": [round(x, 1) for x in e2e_upload],
+                    "stage_ms_per_step": e2e_stage, "search_close_ms": e2e_parts},
+            "steps_ms": [round(x, 1) for x in times],
             "gpu_launches": int(launches), "clocks": clocks}
     if plain is not None:
         line["plain"] = plain

@@ -52,7 +52,8 @@ typedef struct {
   int32_t device;       /* CUDA device ordinal                                       */
   int32_t host_threads; /* host threads for domain definition; 0 = all cores         */
   uint32_t flags;       /* SX_FLAG_*                                                 */
-  int32_t reserved;
+  int32_t pipeline_blocks; /* profile blocks per search whose host domain definition
+                              overlaps the next block's device cascade; 0 = automatic */
   int64_t batch_bytes;  /* device bytes per streamed batch; 0 = 2 GiB                */
 } sx_opts;
 
@@ -150,7 +151,9 @@ void sx_hits_free(sx_hits* h);
  * leaving each stage, DP cells per stage and milliseconds per stage.
  * stage: 0 MSV, 1 bias, 2 Viterbi, 3 Forward pre-screen (device, CUDA
  * events), 4 Forward/Backward row passes of the final pairs (device + copies),
- * 5 host domain definition, 6 whole call (host clock). */
+ * 5 host domain definition (busy time of the host pool, which overlaps the
+ * device stages of later profile blocks), 6 whole call (host clock), 7 host
+ * time after the last device work (the part of stage 5 not hidden). */
 typedef struct {
   int64_t pairs_in[8], pairs_out[8];
   double cells[8];

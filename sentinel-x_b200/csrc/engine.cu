@@ -14,6 +14,8 @@
 //      device Forward/Backward passes that emit the raw special rows of the
 //      final pairs (chunked); host posterior domain definition, envelope
 //      rescoring and reporting on a thread pool.
+// Steps 1-5 run per block of profiles; a block's host domain definition is
+// queued to a background pool and overlaps the device work of later blocks.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,7 +23,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <functional>
 #include <memory>
 #include <mutex>
@@ -69,14 +73,22 @@ template <typename T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  bool owned = true;  // false: a view into memory someone else frees
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p && owned) cudaFree(p);
     p = nullptr;
     n = 0;
+    owned = true;
+  }
+  void view(void* at, size_t count) {
+    release();
+    p = static_cast<T*>(at);
+    n = count;
+    owned = false;
   }
   void alloc(size_t count) {  // grow-only, contents undefined
     if (count <= n && p) return;
@@ -291,6 +303,111 @@ float f32_boundary(Pred pass) {
   return from_ord(hi);
 }
 
+// Device blocks recycled between target sets, so that a caller streaming
+// batches of targets through one engine does not pay a cudaMalloc/cudaFree
+// pair (and the device-wide synchronisation of cudaFree) per batch.
+class BlockPool {
+ public:
+  ~BlockPool() {
+    for (auto& b : free_) cudaFree(b.first);
+  }
+  // A block of at least `bytes`; its size is returned in `got`.
+  void* take(size_t bytes, size_t& got) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      size_t best = free_.size();
+      for (size_t i = 0; i < free_.size(); i++)
+        if (free_[i].second >= bytes && (best == free_.size() || free_[i].second < free_[best].second)) best = i;
+      if (best < free_.size()) {
+        auto b = free_[best];
+        free_.erase(free_.begin() + (std::ptrdiff_t)best);
+        got = b.second;
+        return b.first;
+      }
+    }
+    void* p = nullptr;
+    CK(cudaMalloc(&p, std::max<size_t>(bytes, 256)));
+    got = std::max<size_t>(bytes, 256);
+    return p;
+  }
+  void give(void* p, size_t bytes) {
+    std::lock_guard<std::mutex> g(mu_);
+    free_.emplace_back(p, bytes);
+    if (free_.size() > kKeep) {  // drop the smallest
+      auto it = std::min_element(free_.begin(), free_.end(),
+                                 [](const auto& a, const auto& b) { return a.second < b.second; });
+      cudaFree(it->first);
+      free_.erase(it);
+    }
+  }
+
+ private:
+  static constexpr size_t kKeep = 2;
+  std::mutex mu_;
+  std::vector<std::pair<void*, size_t>> free_;
+};
+
+// A main stream with auxiliary streams that fan out from it and join back
+// into it, all of one scheduling priority.
+struct Streams {
+  static constexpr int kAux = 8;
+  cudaStream_t main = nullptr;
+  cudaStream_t aux[kAux] = {};  // independent launches (shapes, bins) run side by side
+  cudaEvent_t fork_ev = nullptr, join_ev[kAux] = {};
+  void create(int priority) {
+    CK(cudaStreamCreateWithPriority(&main, cudaStreamNonBlocking, priority));
+    for (int a = 0; a < kAux; a++) {
+      CK(cudaStreamCreateWithPriority(&aux[a], cudaStreamNonBlocking, priority));
+      CK(cudaEventCreateWithFlags(&join_ev[a], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+  }
+  void destroy() {
+    if (main) cudaStreamSynchronize(main);
+    for (int a = 0; a < kAux; a++)
+      if (aux[a]) cudaStreamSynchronize(aux[a]);
+    for (int a = 0; a < kAux; a++) {
+      if (aux[a]) cudaStreamDestroy(aux[a]);
+      if (join_ev[a]) cudaEventDestroy(join_ev[a]);
+    }
+    if (fork_ev) cudaEventDestroy(fork_ev);
+    if (main) cudaStreamDestroy(main);
+  }
+};
+
+// Streams, events and survivor lists of one block of a search.  A search
+// keeps two blocks in flight: block b+1's MSV runs on one slot while block
+// b's later stages, row passes and host re-check use the other.  MSV goes to
+// the low-priority streams, everything after it to the high-priority ones,
+// so the short, latency-bound later stages of block b get SMs as soon as
+// block b+1's MSV CTAs retire and MSV fills the rest of the GPU.
+struct Slot {
+  Streams hi, lo;
+  cudaEvent_t ev[8] = {};
+  cudaEvent_t msv_done = nullptr;
+  // grow-only device scratch
+  DevBuf<PairRec> lists[4];
+  DevBuf<BinRegion> bins[4];
+  DevBuf<unsigned> counts;  // 4 stages x kMaxBins
+  DevBuf<unsigned> overflow;
+  DevBuf<MsvTile> tiles;
+  void create() {
+    int least = 0, greatest = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    hi.create(greatest);
+    lo.create(least);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    CK(cudaEventCreateWithFlags(&msv_done, cudaEventDisableTiming));
+  }
+  void destroy() {
+    hi.destroy();
+    lo.destroy();
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (msv_done) cudaEventDestroy(msv_done);
+  }
+};
+
 }  // namespace
 
 // ---- engine objects ----------------------------------------------------------
@@ -300,20 +417,23 @@ struct sx_engine {
   uint32_t flags = 0;
   int64_t batch_bytes = 0;
   int num_sms = 148;
-  cudaStream_t stream = nullptr;
-  static constexpr int kAux = 8;
-  cudaStream_t aux[kAux] = {};  // independent launches (shapes, bins) run side by side
-  cudaEvent_t fork_ev = nullptr, join_ev[kAux] = {};
-  cudaEvent_t ev[8] = {};
+  static constexpr int kAux = Streams::kAux;
+  Slot sl[2];
+  // slot 0 under the names the single-batch entry points use
+  cudaStream_t& stream = sl[0].hi.main;
+  cudaStream_t (&aux)[kAux] = sl[0].hi.aux;
+  cudaEvent_t& fork_ev = sl[0].hi.fork_ev;
+  cudaEvent_t (&join_ev)[kAux] = sl[0].hi.join_ev;
+  cudaEvent_t (&ev)[8] = sl[0].ev;
+  DevBuf<PairRec> (&lists)[4] = sl[0].lists;
+  DevBuf<BinRegion> (&bins)[4] = sl[0].bins;
+  DevBuf<unsigned>& counts = sl[0].counts;
+  DevBuf<unsigned>& overflow = sl[0].overflow;
+  DevBuf<MsvTile>& tiles = sl[0].tiles;
   std::mutex mu;
   sx_search_stats stats{};
-  double host_ms = 0;  // host time inside rows_pass sinks (domain definition)
-  // grow-only device scratch
-  DevBuf<PairRec> lists[4];
-  DevBuf<BinRegion> bins[4];
-  DevBuf<unsigned> counts;   // 4 stages x kNumVbins
-  DevBuf<unsigned> overflow;
-  DevBuf<MsvTile> tiles;
+  int pipeline_blocks = 0;  // profile blocks per search; 0 = by workload size
+  BlockPool target_blocks;  // device memory of freed target sets
   DevBuf<Thresholds> thr;
   DevBuf<float> rows_f, rows_b;
   DevBuf<int64_t> row_off;
@@ -352,6 +472,11 @@ struct sx_targets {
   DevBuf<float4> d_tpar;  // MSV tloop, tmove, null score
   DevBuf<float4> d_xsc;   // multihit loop, move (log), loop, move (prob)
   DevBuf<int32_t> d_order;
+  void* block = nullptr;  // one device block holding all d_* arrays (engine pool)
+  size_t block_bytes = 0;
+  ~sx_targets() {
+    if (block) eng->target_blocks.give(block, block_bytes);
+  }
 };
 
 struct sx_hits {
@@ -363,16 +488,18 @@ namespace {
 
 // Fan independent launches out over the auxiliary streams and join them back
 // into the engine stream.
-void fork_aux(sx_engine* E) {
-  CK(cudaEventRecord(E->fork_ev, E->stream));
-  for (int a = 0; a < sx_engine::kAux; a++) CK(cudaStreamWaitEvent(E->aux[a], E->fork_ev, 0));
+void fork_aux(Streams& X) {
+  CK(cudaEventRecord(X.fork_ev, X.main));
+  for (int a = 0; a < Streams::kAux; a++) CK(cudaStreamWaitEvent(X.aux[a], X.fork_ev, 0));
 }
-void join_aux(sx_engine* E) {
-  for (int a = 0; a < sx_engine::kAux; a++) {
-    CK(cudaEventRecord(E->join_ev[a], E->aux[a]));
-    CK(cudaStreamWaitEvent(E->stream, E->join_ev[a], 0));
+void join_aux(Streams& X) {
+  for (int a = 0; a < Streams::kAux; a++) {
+    CK(cudaEventRecord(X.join_ev[a], X.aux[a]));
+    CK(cudaStreamWaitEvent(X.main, X.join_ev[a], 0));
   }
 }
+void fork_aux(sx_engine* E) { fork_aux(E->sl[0].hi); }
+void join_aux(sx_engine* E) { join_aux(E->sl[0].hi); }
 
 // ---- profile packing --------------------------------------------------------
 void pack_profiles(sx_profiles* P) {
@@ -572,12 +699,28 @@ void pack_targets(sx_targets* T) {
   std::iota(T->order.begin(), T->order.end(), 0);
   std::stable_sort(T->order.begin(), T->order.end(), [&](int a, int b) { return T->len[a] > T->len[b]; });
   cudaStream_t s = T->eng->stream;
-  T->d_res.upload(T->dsq.data(), T->dsq.size(), s);
-  T->d_off.upload(T->off.data(), n, s);
-  T->d_len.upload(T->len.data(), n, s);
-  T->d_tpar.upload(tpar.data(), n, s);
-  T->d_xsc.upload(xsc.data(), n, s);
-  T->d_order.upload(T->order.data(), n, s);
+  // all arrays in one pooled block, each 256-byte aligned
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t o_res = 0, o_off = o_res + up(T->dsq.size()), o_len = o_off + up(8 * n), o_tpar = o_len + up(4 * n);
+  const size_t o_xsc = o_tpar + up(16 * n), o_order = o_xsc + up(16 * n), total = o_order + up(4 * n);
+  if (T->block) T->eng->target_blocks.give(T->block, T->block_bytes);
+  T->block = T->eng->target_blocks.take(total, T->block_bytes);
+  char* b = static_cast<char*>(T->block);
+  T->d_res.view(b + o_res, T->dsq.size());
+  T->d_off.view(b + o_off, n);
+  T->d_len.view(b + o_len, n);
+  T->d_tpar.view(b + o_tpar, n);
+  T->d_xsc.view(b + o_xsc, n);
+  T->d_order.view(b + o_order, n);
+  auto put = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+  };
+  put(T->d_res.p, T->dsq.data(), T->dsq.size());
+  put(T->d_off.p, T->off.data(), 8 * n);
+  put(T->d_len.p, T->len.data(), 4 * n);
+  put(T->d_tpar.p, tpar.data(), 16 * n);
+  put(T->d_xsc.p, xsc.data(), 16 * n);
+  put(T->d_order.p, T->order.data(), 4 * n);
   CK(cudaStreamSynchronize(s));
 }
 
@@ -647,11 +790,19 @@ struct FinalPair {
   int32_t slot;
 };
 
+// Host copies of one chunk of raw Forward/Backward special rows.
+struct RowsChunk {
+  std::vector<float> f, b;    // rows of every pair of the chunk, back to back
+  std::vector<int64_t> off;   // offset of pair q's rows in f and b
+  std::vector<size_t> which;  // pair q's index in the caller's list
+};
+
 // Device Forward and Backward with row output for `pairs`, in chunks bounded
-// by `row_budget` floats per direction; calls sink(i, fwd_rows, bwd_rows).
-template <typename Sink>
-void rows_pass(sx_engine* E, const sx_profiles* P, const sx_targets* T, const std::vector<FinalPair>& pairs,
-               Sink&& sink) {
+// by `row_budget` floats per direction; hands each chunk's host copy to
+// consume(RowsChunk&&) as soon as it has arrived.
+template <typename Consume>
+void rows_pass(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T, const std::vector<FinalPair>& pairs,
+               Consume&& consume) {
   if (pairs.empty()) return;
   const auto& K = kernels();
   const int64_t row_budget = std::max<int64_t>(E->batch_bytes / 2 / (int64_t)sizeof(float), 1 << 20);
@@ -670,10 +821,9 @@ void rows_pass(sx_engine* E, const sx_profiles* P, const sx_targets* T, const st
     std::vector<std::vector<size_t>> byb(kNumVbins);
     for (size_t i = i0; i < i1; i++) byb[P->dp[pairs[i].p].vbin].push_back(i);
     std::vector<PairRec> recs;
-    std::vector<int64_t> roff;
+    RowsChunk c;
     std::vector<BinRegion> reg(kNumVbins);
     std::vector<unsigned> cnt(kNumVbins, 0);
-    std::vector<size_t> which;
     int64_t ro = 0;
     for (int b = 0; b < kNumVbins; b++) {
       reg[b].off = (int64_t)recs.size();
@@ -684,49 +834,108 @@ void rows_pass(sx_engine* E, const sx_profiles* P, const sx_targets* T, const st
         const FinalPair& f = pairs[i];
         PairRec r{f.p, f.t, f.usc, f.filtersc, f.vsc, 0.f, f.slot, 0};
         recs.push_back(r);
-        roff.push_back(ro);
-        which.push_back(i);
+        c.off.push_back(ro);
+        c.which.push_back(i);
         ro += 6 * ((int64_t)T->len[f.t] + 1);
       }
     }
-    cudaStream_t s = E->stream;
-    E->lists[3].upload(recs.data(), recs.size(), s);
-    E->row_off.upload(roff.data(), roff.size(), s);
-    E->bins[3].upload(reg.data(), reg.size(), s);
-    E->counts.alloc(4 * kMaxBins);
-    CK(cudaMemcpyAsync(E->counts.p + 3 * kMaxBins, cnt.data(), sizeof(unsigned) * kNumVbins, cudaMemcpyHostToDevice, s));
+    cudaStream_t s = S.hi.main;
+    S.lists[3].upload(recs.data(), recs.size(), s);
+    E->row_off.upload(c.off.data(), c.off.size(), s);
+    S.bins[3].upload(reg.data(), reg.size(), s);
+    S.counts.alloc(4 * kMaxBins);
+    CK(cudaMemcpyAsync(S.counts.p + 3 * kMaxBins, cnt.data(), sizeof(unsigned) * kNumVbins, cudaMemcpyHostToDevice, s));
     E->rows_f.alloc((size_t)ro);
     E->rows_b.alloc((size_t)ro);
     // rows the kernels never touch are zero
     CK(cudaMemsetAsync(E->rows_f.p, 0, sizeof(float) * (size_t)ro, s));
     CK(cudaMemsetAsync(E->rows_b.p, 0, sizeof(float) * (size_t)ro, s));
-    fork_aux(E);
+    fork_aux(S.hi);
     for (int b = 0; b < kNumVbins; b++) {
       if (!cnt[b]) continue;
       const int blocks = (int)std::min<int64_t>((cnt[b] + 7) / 8, (int64_t)E->num_sms * 16);
-      cudaStream_t sa = E->aux[(2 * b) % sx_engine::kAux], sb = E->aux[(2 * b + 1) % sx_engine::kAux];
-      K.fwd[b]<<<blocks, 256, 0, sa>>>(E->lists[3].p, E->counts.p + 3 * kMaxBins, E->bins[3].p, b, nullptr, nullptr,
-                                       nullptr, E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p,
+      cudaStream_t sa = S.hi.aux[(2 * b) % Streams::kAux], sb = S.hi.aux[(2 * b + 1) % Streams::kAux];
+      K.fwd[b]<<<blocks, 256, 0, sa>>>(S.lists[3].p, S.counts.p + 3 * kMaxBins, S.bins[3].p, b, nullptr, nullptr,
+                                       nullptr, S.overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p,
                                        T->d_off.p, T->d_len.p, T->d_xsc.p, 0.f, E->rows_f.p, E->row_off.p);
-      K.bwd[b]<<<blocks, 256, 0, sb>>>(E->lists[3].p, E->counts.p + 3 * kMaxBins, E->bins[3].p, b, P->d_prof.p,
+      K.bwd[b]<<<blocks, 256, 0, sb>>>(S.lists[3].p, S.counts.p + 3 * kMaxBins, S.bins[3].p, b, P->d_prof.p,
                                        P->d_vfb.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p, E->rows_b.p,
                                        E->row_off.p);
       E->stats.kernel_launches += 2;
     }
     CK(cudaGetLastError());
-    join_aux(E);
-    std::vector<float> hf((size_t)ro), hb((size_t)ro);
-    CK(cudaMemcpyAsync(hf.data(), E->rows_f.p, sizeof(float) * (size_t)ro, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(hb.data(), E->rows_b.p, sizeof(float) * (size_t)ro, cudaMemcpyDeviceToHost, s));
+    join_aux(S.hi);
+    c.f.resize((size_t)ro);
+    c.b.resize((size_t)ro);
+    CK(cudaMemcpyAsync(c.f.data(), E->rows_f.p, sizeof(float) * (size_t)ro, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(c.b.data(), E->rows_b.p, sizeof(float) * (size_t)ro, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    const auto t_host = std::chrono::steady_clock::now();
-    parallel_for(which.size(), E->host_threads, [&](size_t q) {
-      sink(which[q], hf.data() + roff[q], hb.data() + roff[q]);
-    });
-    E->host_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host).count();
+    consume(std::move(c));
     i0 = i1;
   }
 }
+
+// rows_pass with each chunk consumed on the calling thread: sink(i, fwd_rows,
+// bwd_rows) for every pair, spread over the engine's host threads.
+template <typename Sink>
+void rows_pass_sync(sx_engine* E, const sx_profiles* P, const sx_targets* T, const std::vector<FinalPair>& pairs,
+                    Sink&& sink) {
+  rows_pass(E, E->sl[0], P, T, pairs, [&](RowsChunk&& c) {
+    parallel_for(c.which.size(), E->host_threads,
+                 [&](size_t q) { sink(c.which[q], c.f.data() + c.off[q], c.b.data() + c.off[q]); });
+  });
+}
+
+// Background host work: one driver thread runs the queued jobs in order, each
+// over `threads` workers, while the engine thread keeps the device busy with
+// later profile blocks.
+class HostQueue {
+ public:
+  explicit HostQueue(int threads) : threads_(std::max(1, threads)), th_([this] { loop(); }) {}
+  ~HostQueue() { finish(); }
+  void push(std::function<void(int)> job) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      q_.push_back(std::move(job));
+    }
+    cv_.notify_one();
+  }
+  // Runs what is queued to completion and stops the driver; returns its busy
+  // milliseconds.
+  double finish() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      done_ = true;
+    }
+    cv_.notify_one();
+    if (th_.joinable()) th_.join();
+    return busy_ms_;
+  }
+
+ private:
+  void loop() {
+    for (;;) {
+      std::function<void(int)> job;
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        cv_.wait(g, [&] { return done_ || !q_.empty(); });
+        if (q_.empty()) return;
+        job = std::move(q_.front());
+        q_.pop_front();
+      }
+      const auto t0 = std::chrono::steady_clock::now();
+      job(threads_);
+      busy_ms_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+  }
+  const int threads_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<std::function<void(int)>> q_;
+  bool done_ = false;
+  double busy_ms_ = 0;
+  std::thread th_;  // last member: starts once the others exist
+};
 
 struct PairResult {
   bool hit = false;
@@ -807,11 +1016,13 @@ int check_cutoffs(const sx_profiles* P, int kind) {
 
 // MSV tiles: for every profile, slices of the length-sorted target order with
 // roughly equal residue counts.
-std::vector<std::vector<MsvTile>> make_all_pairs_tiles(const sx_engine* E, const sx_profiles* P, const sx_targets* T) {
+// MSV tiles of every (profile in [p0, p1), target) pair, grouped by kernel shape.
+std::vector<std::vector<MsvTile>> make_all_pairs_tiles(const sx_engine* E, const sx_profiles* P, const sx_targets* T,
+                                                       int p0, int p1) {
   std::vector<std::vector<MsvTile>> by_shape(kNumMsvShapes);
   const int nt = (int)T->len.size();
-  if (nt == 0) return by_shape;
-  const int np = (int)P->h.size();
+  if (nt == 0 || p1 <= p0) return by_shape;
+  const int np = p1 - p0;
   const int waves = 16;
   int nslices = (int)std::ceil((double)waves * E->num_sms * 2 / std::max(1, np));
   nslices = std::max(1, std::min(nslices, std::max(1, nt / 32)));
@@ -827,7 +1038,7 @@ std::vector<std::vector<MsvTile>> make_all_pairs_tiles(const sx_engine* E, const
     }
   }
   std::vector<int> pord(np);
-  std::iota(pord.begin(), pord.end(), 0);
+  std::iota(pord.begin(), pord.end(), p0);
   std::stable_sort(pord.begin(), pord.end(), [&](int a, int b) { return P->h[a].m > P->h[b].m; });
   for (int pi : pord)
     for (int s = 0; s < nslices; s++)
@@ -835,7 +1046,7 @@ std::vector<std::vector<MsvTile>> make_all_pairs_tiles(const sx_engine* E, const
   return by_shape;
 }
 
-void launch_msv(sx_engine* E, const sx_profiles* P, const sx_targets* T, const std::vector<std::vector<MsvTile>>& tiles,
+void launch_msv(sx_engine* E, Slot& S, Streams& X, const sx_profiles* P, const sx_targets* T, const std::vector<std::vector<MsvTile>>& tiles,
                 const int32_t* d_list, float* d_scores, const int32_t* d_slot, PairRec* surv, const BinRegion* bins,
                 unsigned* counts) {
   const auto& K = kernels();
@@ -847,7 +1058,7 @@ void launch_msv(sx_engine* E, const sx_profiles* P, const sx_targets* T, const s
   }
   start[kNumMsvShapes] = all.size();
   if (all.empty()) return;
-  E->tiles.upload(all.data(), all.size(), E->stream);
+  S.tiles.upload(all.data(), all.size(), X.main);
   // biggest launches first, each on its own auxiliary stream
   std::vector<int> order;
   for (int s = 0; s < kNumMsvShapes; s++)
@@ -856,7 +1067,7 @@ void launch_msv(sx_engine* E, const sx_profiles* P, const sx_targets* T, const s
   for (int s : order)
     for (size_t q = start[s]; q < start[s + 1]; q++) work[s] += (double)all[q].end - all[q].begin;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
-  fork_aux(E);
+  fork_aux(X);
   int lane = 0;
   for (int s : order) {
     const size_t nt = start[s + 1] - start[s];
@@ -865,42 +1076,42 @@ void launch_msv(sx_engine* E, const sx_profiles* P, const sx_targets* T, const s
     const size_t rowp = ((size_t)(c / 4) * g + 7) & ~(size_t)7;
     const size_t smem = (size_t)ncopy * (25 * rowp + 8 + g) * sizeof(float4);
     CK(cudaFuncSetAttribute((const void*)K.msv[s], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    K.msv[s]<<<(unsigned)nt, 256, smem, E->aux[lane++ % sx_engine::kAux]>>>(
-        E->tiles.p + start[s], P->d_prof.p, E->thr.p, P->d_msv.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_tpar.p,
-        d_list, d_scores, d_slot, surv, bins, counts, E->overflow.p);
+    K.msv[s]<<<(unsigned)nt, 256, smem, X.aux[lane++ % Streams::kAux]>>>(
+        S.tiles.p + start[s], P->d_prof.p, E->thr.p, P->d_msv.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_tpar.p,
+        d_list, d_scores, d_slot, surv, bins, counts, S.overflow.p);
     E->stats.kernel_launches++;
   }
   CK(cudaGetLastError());
-  join_aux(E);
+  join_aux(X);
 }
 
 // One filter stage over per-vbin lists: stage `si` reads lists[si] and writes lists[si+1].
-void launch_stage(sx_engine* E, const sx_profiles* P, const sx_targets* T, int si, const std::vector<unsigned>& nin) {
+void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T, int si, const std::vector<unsigned>& nin) {
   const auto& K = kernels();
-  cudaStream_t s = E->stream;
-  unsigned* cin = E->counts.p + si * kMaxBins;
-  unsigned* cout = E->counts.p + (si + 1) * kMaxBins;
+  cudaStream_t s = S.hi.main;
+  unsigned* cin = S.counts.p + si * kMaxBins;
+  unsigned* cout = S.counts.p + (si + 1) * kMaxBins;
   if (si == 0) {
     unsigned mx = 0;
     for (int b = 0; b < kNumVbins; b++) mx = std::max(mx, nin[b]);
     if (!mx) return;
     dim3 grid((unsigned)std::min<int64_t>((mx + 255) / 256, (int64_t)E->num_sms * 8), kNumVbins);
-    sxk::bias_kernel<<<grid, 256, 0, s>>>(E->lists[0].p, cin, E->bins[0].p, E->lists[1].p, E->bins[1].p, cout,
-                                          E->overflow.p, P->d_bias.p, E->thr.p, T->d_res.p, T->d_off.p, T->d_len.p,
+    sxk::bias_kernel<<<grid, 256, 0, s>>>(S.lists[0].p, cin, S.bins[0].p, S.lists[1].p, S.bins[1].p, cout,
+                                          S.overflow.p, P->d_bias.p, E->thr.p, T->d_res.p, T->d_off.p, T->d_len.p,
                                           kSlackBits, nullptr, P->d_prof.p);
     E->stats.kernel_launches++;
   } else {
-    fork_aux(E);
+    fork_aux(S.hi);
     int lane = 0;
     const int nb = si == 1 ? kNumVitShapes : kNumVbins;
     for (int b = 0; b < nb; b++) {
       if (!nin[b]) continue;
       const int blocks = (int)std::min<int64_t>((nin[b] + 7) / 8, (int64_t)E->num_sms * 16);
-      cudaStream_t s = E->aux[lane++ % sx_engine::kAux];
+      cudaStream_t s = S.hi.aux[lane++ % Streams::kAux];
       if (si == 1 && (E->flags & SX_FLAG_PLAIN)) {
         sxk::plain_viterbi_kernel<<<(unsigned)std::min<int64_t>(nin[b], (int64_t)E->num_sms * 64), sxk::kPlainThreads,
-                                    0, E->stream>>>(E->lists[1].p, cin, E->bins[1].p, b, E->lists[2].p, E->bins[2].p,
-                                                    cout, E->overflow.p, P->d_pprof.p, P->d_plain.p, E->thr.p,
+                                    0, S.hi.main>>>(S.lists[1].p, cin, S.bins[1].p, b, S.lists[2].p, S.bins[2].p,
+                                                    cout, S.overflow.p, P->d_pprof.p, P->d_plain.p, E->thr.p,
                                                     T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p, kSlackBits,
                                                     P->d_prof.p);
         E->stats.kernel_launches++;
@@ -909,16 +1120,16 @@ void launch_stage(sx_engine* E, const sx_profiles* P, const sx_targets* T, int s
       if (si == 1) {
         const int g = kVitShapes[b].g;
         const int vblocks = (int)std::min<int64_t>(((int64_t)nin[b] * g + 255) / 256, (int64_t)E->num_sms * 16);
-        K.vitg[b]<<<vblocks, 256, 0, s>>>(E->lists[1].p, cin, E->bins[1].p, b, E->lists[2].p, E->bins[2].p, cout,
-                                          E->overflow.p, P->d_prof.p, E->thr.p, P->d_vit.p, T->d_res.p, T->d_off.p,
+        K.vitg[b]<<<vblocks, 256, 0, s>>>(S.lists[1].p, cin, S.bins[1].p, b, S.lists[2].p, S.bins[2].p, cout,
+                                          S.overflow.p, P->d_prof.p, E->thr.p, P->d_vit.p, T->d_res.p, T->d_off.p,
                                           T->d_len.p, T->d_xsc.p, kSlackBits, nullptr);
       } else
-        K.fwd[b]<<<blocks, 256, 0, s>>>(E->lists[2].p, cin, E->bins[2].p, b, E->lists[3].p, E->bins[3].p, cout,
-                                        E->overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
+        K.fwd[b]<<<blocks, 256, 0, s>>>(S.lists[2].p, cin, S.bins[2].p, b, S.lists[3].p, S.bins[3].p, cout,
+                                        S.overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
                                         T->d_len.p, T->d_xsc.p, kSlackBits, nullptr, nullptr);
       E->stats.kernel_launches++;
     }
-    join_aux(E);
+    join_aux(S.hi);
   }
   CK(cudaGetLastError());
 }
@@ -929,11 +1140,187 @@ double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
+// Contiguous ranges of profile indices with about equal filtered DP cells.
+// Each range runs through the device cascade as one block; the host domain
+// definition of a block overlaps the device work of the blocks after it.
+std::vector<std::pair<int, int>> profile_blocks(const sx_engine* E, const sx_profiles* P, const sx_targets* T,
+                                                const std::vector<Thresholds>& th) {
+  constexpr double kCellsPerBlock = 2.5e11;  // ~80 ms of B200 cascade
+  constexpr int kMaxBlocks = 8;
+  const int np = (int)P->h.size();
+  std::vector<double> w(np, 0.0);
+  double total = 0;
+  int nfilt = 0;
+  for (int pi = 0; pi < np; pi++)
+    if (th[pi].exact) {
+      w[pi] = (double)std::max(P->h[pi].m, 1) * std::max(T->residues, 1.0);
+      total += w[pi];
+      nfilt++;
+    }
+  std::vector<std::pair<int, int>> out;
+  if (nfilt == 0 || T->len.empty()) return out;
+  int nb = E->pipeline_blocks > 0 ? E->pipeline_blocks
+                                  : (int)std::min<double>(kMaxBlocks, std::max(1.0, std::floor(total / kCellsPerBlock)));
+  nb = std::max(1, std::min(nb, nfilt));
+  int p0 = 0;
+  double acc = 0;
+  for (int pi = 0; pi < np; pi++) {
+    acc += w[pi];
+    if ((int)out.size() < nb - 1 && acc >= total * (double)(out.size() + 1) / nb) {
+      out.emplace_back(p0, pi + 1);
+      p0 = pi + 1;
+    }
+  }
+  if (p0 < np) out.emplace_back(p0, np);
+  return out;
+}
+
+// One block of filtered profiles [p0, p1) going through the device cascade.
+struct BlockRun {
+  int p0 = 0, p1 = 0;
+  int attempt = 0;  // survivor-list sizing attempt; lists grow 4x per overflow
+  StageLists L[4];
+  std::vector<double> pairs_in_bin, pairs_in_vs;
+  double cells_total = 0;
+};
+constexpr int kListAttempts = 4;
+
+// Sizes the block's survivor lists, clears its counters and queues its MSV on
+// slot S; returns without waiting for the device.
+void cascade_launch(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T,
+                    const std::vector<Thresholds>& th, BlockRun& R) {
+  const size_t nt = T->len.size();
+  cudaStream_t s = S.lo.main;
+  if (R.attempt == 0) {  // capacity per bin from the number of pairs it holds
+    R.pairs_in_bin.assign(kMaxBins, 0.0);
+    R.pairs_in_vs.assign(kMaxBins, 0.0);
+    R.cells_total = 0;
+    for (int pi = R.p0; pi < R.p1; pi++)
+      if (th[pi].exact) {
+        R.pairs_in_bin[P->dp[pi].vbin] += (double)nt;
+        R.pairs_in_vs[P->dp[pi].vshape] += (double)nt;
+        R.cells_total += (double)P->h[pi].m * T->residues;
+      }
+  }
+  // the last attempt sizes every list for all of its pairs and cannot overflow
+  const bool full = R.attempt >= kListAttempts - 1;
+  const double scale = std::pow(4.0, (double)R.attempt);
+  std::vector<double> w1(kMaxBins), w1v(kMaxBins), w3(kMaxBins);
+  for (int b = 0; b < kMaxBins; b++) {
+    const double pb = R.pairs_in_bin[b], pv = R.pairs_in_vs[b];
+    w1[b] = full ? pb : std::min(pb, scale * (0.06 * pb + 8192));
+    w1v[b] = full ? pv : std::min(pv, scale * (0.06 * pv + 8192));
+    w3[b] = full ? pb : std::min(pb, scale * (0.01 * pb + 4096));
+  }
+  R.L[0] = make_regions(w1);
+  R.L[1] = make_regions(w1v);
+  R.L[2] = make_regions(w3);
+  R.L[3] = make_regions(w3);
+  for (int q = 0; q < 4; q++) {
+    S.lists[q].alloc((size_t)R.L[q].total);
+    S.bins[q].upload(R.L[q].reg.data(), kMaxBins, s);
+  }
+  CK(cudaMemsetAsync(S.counts.p, 0, sizeof(unsigned) * 4 * kMaxBins, s));
+  CK(cudaMemsetAsync(S.overflow.p, 0, sizeof(unsigned), s));
+  // stage 0: MSV over all pairs of the block's filtered profiles
+  CK(cudaEventRecord(S.ev[0], s));
+  if (E->flags & SX_FLAG_PLAIN) {
+    const int64_t last = (int64_t)R.p1 * (int64_t)nt;
+    for (int64_t first = (int64_t)R.p0 * (int64_t)nt; first < last; first += (1LL << 30)) {
+      const int64_t n = std::min<int64_t>(last - first, 1LL << 30);
+      sxk::plain_msv_kernel<<<(unsigned)n, sxk::kPlainThreads, 0, s>>>(
+          first, (int)nt, P->d_pprof.p, P->d_plain.p, P->d_prof.p, E->thr.p, T->d_res.p, T->d_off.p, T->d_len.p,
+          T->d_tpar.p, S.lists[0].p, S.bins[0].p, S.counts.p, S.overflow.p);
+      E->stats.kernel_launches++;
+    }
+    CK(cudaGetLastError());
+  } else {
+    auto tiles = make_all_pairs_tiles(E, P, T, R.p0, R.p1);
+    for (auto& v : tiles)
+      v.erase(std::remove_if(v.begin(), v.end(), [&](const MsvTile& t) { return !th[t.p].exact; }), v.end());
+    launch_msv(E, S, S.lo, P, T, tiles, T->d_order.p, nullptr, nullptr, S.lists[0].p, S.bins[0].p, S.counts.p);
+  }
+  CK(cudaEventRecord(S.ev[1], s));
+  CK(cudaEventRecord(S.msv_done, s));
+}
+
+// Drives the block's bias, Viterbi and Forward pre-screen stages on slot S,
+// then gathers the survivors and re-checks them exactly on the host, appending
+// the pairs that pass to `finals`.  Returns false if a survivor list
+// overflowed; the caller then relaunches the block (with larger lists).
+bool cascade_finish(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T,
+                    const std::vector<Thresholds>& th, const SearchOpts& o, BlockRun& R,
+                    std::vector<FinalPair>& finals) {
+  cudaStream_t s = S.hi.main;
+  CK(cudaStreamWaitEvent(s, S.msv_done, 0));
+  std::vector<unsigned> cnt(4 * kMaxBins);
+  for (int si = 0; si < 3; si++) {
+    CK(cudaMemcpyAsync(cnt.data(), S.counts.p, sizeof(unsigned) * 4 * kMaxBins, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    std::vector<unsigned> nin(kMaxBins);
+    for (int b = 0; b < kMaxBins; b++) nin[b] = std::min(cnt[si * kMaxBins + b], R.L[si].reg[b].cap);
+    CK(cudaEventRecord(S.ev[2 + si], s));
+    launch_stage(E, S, P, T, si, nin);
+  }
+  CK(cudaEventRecord(S.ev[5], s));
+  unsigned ovf = 0;
+  CK(cudaMemcpyAsync(cnt.data(), S.counts.p, sizeof(unsigned) * 4 * kMaxBins, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&ovf, S.overflow.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (ovf && R.attempt < kListAttempts - 1) {  // a survivor list was too small
+    R.attempt++;
+    return false;
+  }
+  // stats
+  double pairs_all = 0;
+  for (int b = 0; b < kMaxBins; b++) pairs_all += R.pairs_in_bin[b];
+  E->stats.pairs_in[0] += (int64_t)pairs_all;
+  E->stats.cells[0] += R.cells_total;
+  for (int si = 0; si < 4; si++) {
+    int64_t c = 0;
+    for (int b = 0; b < kMaxBins; b++) c += cnt[si * kMaxBins + b];
+    E->stats.pairs_out[si] += c;
+    if (si < 3) E->stats.pairs_in[si + 1] += c;
+  }
+  E->stats.ms[0] += elapsed_ms(S.ev[0], S.ev[1]);
+  E->stats.ms[1] += elapsed_ms(S.ev[2], S.ev[3]);
+  E->stats.ms[2] += elapsed_ms(S.ev[3], S.ev[4]);
+  E->stats.ms[3] += elapsed_ms(S.ev[4], S.ev[5]);
+  // gather stage-3 survivors
+  std::vector<PairRec> surv;
+  for (int b = 0; b < kNumVbins; b++) {
+    const unsigned n = std::min(cnt[3 * kMaxBins + b], R.L[3].reg[b].cap);
+    if (!n) continue;
+    const size_t o0 = surv.size();
+    surv.resize(o0 + n);
+    CK(cudaMemcpyAsync(surv.data() + o0, S.lists[3].p + R.L[3].reg[b].off, sizeof(PairRec) * n,
+                       cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  // exact host re-check of F1 / bias / F2 with the reference's libm
+  std::vector<char> keep(surv.size(), 0);
+  parallel_for(surv.size(), E->host_threads, [&](size_t i) {
+    PairRec& r = surv[i];
+    const ProfileHost& h = P->h[r.p];
+    const uint8_t* d = T->dsq.data() + T->off[r.t];
+    const int64_t l = T->len[r.t];
+    const float nullsc = null1_score(l);
+    if (gumbel_survival((double)((r.usc - nullsc) / kLn2f), h.msv[0], h.msv[1]) > o.f1) return;
+    const float fsc = composition_bias_score(h, d, l);
+    r.filtersc = fsc;
+    if (gumbel_survival((double)((r.usc - fsc) / kLn2f), h.msv[0], h.msv[1]) > o.f1) return;
+    if (gumbel_survival((double)((r.vsc - fsc) / kLn2f), h.vit[0], h.vit[1]) > o.f2) return;
+    keep[i] = 1;
+  });
+  for (size_t i = 0; i < surv.size(); i++)
+    if (keep[i]) finals.push_back({surv[i].p, surv[i].t, surv[i].usc, surv[i].filtersc, surv[i].vsc, -1});
+  return true;
+}
+
 int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx_search_cfg* cfg, sx_hits* out) {
   int rc = check_cutoffs(P, cfg->cutoff_kind);
   if (rc) return rc;
   E->stats = sx_search_stats{};
-  E->host_ms = 0;
   SearchOpts o;
   o.filters = cfg->filters != 0;
   o.null2 = cfg->null2 != 0;
@@ -944,137 +1331,25 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
   cudaStream_t s = E->stream;
   std::vector<Thresholds> th = make_thresholds(P->h, o);
   E->thr.upload(th.data(), th.size(), s);
-  E->overflow.alloc(1);
-  E->counts.alloc(4 * kMaxBins);
-  std::vector<FinalPair> finals;
-  auto t_start = std::chrono::steady_clock::now();
-
-  // Profiles searched with filters vs. without (uncalibrated or --max): the
-  // latter send every target straight to Forward/Backward.
-  std::vector<int> unfiltered;
-  for (size_t pi = 0; pi < np; pi++)
-    if (!th[pi].exact) unfiltered.push_back((int)pi);
-  const bool any_filtered = unfiltered.size() < np;
-
-  if (any_filtered && nt > 0) {
-    // capacity per vbin from the number of pairs it holds
-    std::vector<double> pairs_in_bin(kMaxBins, 0.0), pairs_in_vs(kMaxBins, 0.0);
-    double cells_total = 0;
-    for (size_t pi = 0; pi < np; pi++)
-      if (th[pi].exact) {
-        pairs_in_bin[P->dp[pi].vbin] += (double)nt;
-        pairs_in_vs[P->dp[pi].vshape] += (double)nt;
-        cells_total += (double)P->h[pi].m * T->residues;
-      }
-    double scale = 1.0;
-    for (int attempt = 0; attempt < 4; attempt++) {
-      std::vector<double> w1(kMaxBins), w1v(kMaxBins), w3(kMaxBins);
-      for (int b = 0; b < kMaxBins; b++) {
-        w1[b] = pairs_in_bin[b] > 0 ? std::min(pairs_in_bin[b], scale * (0.06 * pairs_in_bin[b] + 8192)) : 0;
-        w1v[b] = pairs_in_vs[b] > 0 ? std::min(pairs_in_vs[b], scale * (0.06 * pairs_in_vs[b] + 8192)) : 0;
-        w3[b] = pairs_in_bin[b] > 0 ? std::min(pairs_in_bin[b], scale * (0.01 * pairs_in_bin[b] + 4096)) : 0;
-      }
-      StageLists L0 = make_regions(w1), L1 = make_regions(w1v), L2 = make_regions(w3), L3 = make_regions(w3);
-      StageLists* Ls[4] = {&L0, &L1, &L2, &L3};
-      for (int q = 0; q < 4; q++) {
-        E->lists[q].alloc((size_t)Ls[q]->total);
-        E->bins[q].upload(Ls[q]->reg.data(), kMaxBins, s);
-      }
-      CK(cudaMemsetAsync(E->counts.p, 0, sizeof(unsigned) * 4 * kMaxBins, s));
-      CK(cudaMemsetAsync(E->overflow.p, 0, sizeof(unsigned), s));
-      // stage 0: MSV over all pairs of filtered profiles
-      auto tiles = make_all_pairs_tiles(E, P, T);
-      for (auto& v : tiles)
-        v.erase(std::remove_if(v.begin(), v.end(), [&](const MsvTile& t) { return !th[t.p].exact; }), v.end());
-      CK(cudaEventRecord(E->ev[0], s));
-      if (E->flags & SX_FLAG_PLAIN) {
-        const int64_t total = (int64_t)np * (int64_t)nt;
-        for (int64_t first = 0; first < total; first += (1LL << 30)) {
-          const int64_t n = std::min<int64_t>(total - first, 1LL << 30);
-          sxk::plain_msv_kernel<<<(unsigned)n, sxk::kPlainThreads, 0, s>>>(
-              first, (int)nt, P->d_pprof.p, P->d_plain.p, P->d_prof.p, E->thr.p, T->d_res.p, T->d_off.p,
-              T->d_len.p, T->d_tpar.p, E->lists[0].p, E->bins[0].p, E->counts.p, E->overflow.p);
-          E->stats.kernel_launches++;
-        }
-        CK(cudaGetLastError());
-      } else {
-        launch_msv(E, P, T, tiles, T->d_order.p, nullptr, nullptr, E->lists[0].p, E->bins[0].p, E->counts.p);
-      }
-      CK(cudaEventRecord(E->ev[1], s));
-      std::vector<unsigned> cnt(4 * kMaxBins);
-      for (int si = 0; si < 3; si++) {
-        CK(cudaMemcpyAsync(cnt.data(), E->counts.p, sizeof(unsigned) * 4 * kMaxBins, cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        std::vector<unsigned> nin(kMaxBins);
-        for (int b = 0; b < kMaxBins; b++) nin[b] = std::min(cnt[si * kMaxBins + b], Ls[si]->reg[b].cap);
-        CK(cudaEventRecord(E->ev[2 + si], s));
-        launch_stage(E, P, T, si, nin);
-      }
-      CK(cudaEventRecord(E->ev[5], s));
-      unsigned ovf = 0;
-      CK(cudaMemcpyAsync(cnt.data(), E->counts.p, sizeof(unsigned) * 4 * kMaxBins, cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpyAsync(&ovf, E->overflow.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      if (ovf) {  // a survivor list was too small: grow and rerun
-        scale *= 4.0;
-        continue;
-      }
-      // stats
-      double pairs_all = 0;
-      for (int b = 0; b < kMaxBins; b++) pairs_all += pairs_in_bin[b];
-      E->stats.pairs_in[0] = (int64_t)pairs_all;
-      E->stats.cells[0] = cells_total;
-      for (int si = 0; si < 4; si++) {
-        int64_t c = 0;
-        for (int b = 0; b < kMaxBins; b++) c += cnt[si * kMaxBins + b];
-        E->stats.pairs_out[si] = c;
-        if (si < 3) E->stats.pairs_in[si + 1] = c;
-      }
-      E->stats.ms[0] = elapsed_ms(E->ev[0], E->ev[1]);
-      E->stats.ms[1] = elapsed_ms(E->ev[2], E->ev[3]);
-      E->stats.ms[2] = elapsed_ms(E->ev[3], E->ev[4]);
-      E->stats.ms[3] = elapsed_ms(E->ev[4], E->ev[5]);
-      // gather stage-3 survivors
-      std::vector<PairRec> surv;
-      for (int b = 0; b < kNumVbins; b++) {
-        const unsigned n = std::min(cnt[3 * kMaxBins + b], L3.reg[b].cap);
-        if (!n) continue;
-        const size_t o0 = surv.size();
-        surv.resize(o0 + n);
-        CK(cudaMemcpyAsync(surv.data() + o0, E->lists[3].p + L3.reg[b].off, sizeof(PairRec) * n,
-                           cudaMemcpyDeviceToHost, s));
-      }
-      CK(cudaStreamSynchronize(s));
-      // exact host re-check of F1 / bias / F2 with the reference's libm
-      std::vector<char> keep(surv.size(), 0);
-      parallel_for(surv.size(), E->host_threads, [&](size_t i) {
-        PairRec& r = surv[i];
-        const ProfileHost& h = P->h[r.p];
-        const uint8_t* d = T->dsq.data() + T->off[r.t];
-        const int64_t l = T->len[r.t];
-        const float nullsc = null1_score(l);
-        if (gumbel_survival((double)((r.usc - nullsc) / kLn2f), h.msv[0], h.msv[1]) > o.f1) return;
-        const float fsc = composition_bias_score(h, d, l);
-        r.filtersc = fsc;
-        if (gumbel_survival((double)((r.usc - fsc) / kLn2f), h.msv[0], h.msv[1]) > o.f1) return;
-        if (gumbel_survival((double)((r.vsc - fsc) / kLn2f), h.vit[0], h.vit[1]) > o.f2) return;
-        keep[i] = 1;
-      });
-      for (size_t i = 0; i < surv.size(); i++)
-        if (keep[i]) finals.push_back({surv[i].p, surv[i].t, surv[i].usc, surv[i].filtersc, surv[i].vsc, -1});
-      break;
-    }
+  for (Slot& S : E->sl) {
+    S.overflow.alloc(1);
+    S.counts.alloc(4 * kMaxBins);
   }
-  for (int pi : unfiltered)
-    for (size_t t = 0; t < nt; t++) finals.push_back({pi, (int32_t)t, 0.f, 0.f, 0.f, -1});
-  E->stats.pairs_in[4] = (int64_t)finals.size();
+  const auto t_start = std::chrono::steady_clock::now();
 
-  // Forward/Backward rows + host domain definition
-  std::vector<PairResult> res(finals.size());
+  // Profiles searched with filters go through the cascade in blocks; those
+  // without (uncalibrated, or --max) send every target straight to
+  // Forward/Backward as a last block.
+  struct BlockOut {
+    std::vector<FinalPair> finals;
+    std::vector<PairResult> res;
+  };
+  std::vector<std::unique_ptr<BlockOut>> outs;
   std::atomic<int64_t> n_domain{0};
-  auto t_rows = std::chrono::steady_clock::now();
-  rows_pass(E, P, T, finals, [&](size_t i, const float* fr, const float* br) {
-    const FinalPair& f = finals[i];
+  double rows_ms = 0;
+  // F3 and domain definition of one final pair (pipeline.rs:179-293)
+  auto define_pair = [&](BlockOut* B, size_t i, const float* fr, const float* br) {
+    const FinalPair& f = B->finals[i];
     const ProfileHost& h = P->h[f.p];
     const int64_t l = T->len[f.t];
     const float fwdsc = forward_score_from_rows(h, l, fr);
@@ -1083,19 +1358,84 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     }
     n_domain++;
     RawRows rr{fr, br};
-    res[i].hit = define_domains(h, T->dsq.data() + T->off[f.t], l, rr, fwdsc, o, res[i].h);
-  });
-  auto t_end = std::chrono::steady_clock::now();
+    B->res[i].hit = define_domains(h, T->dsq.data() + T->off[f.t], l, rr, fwdsc, o, B->res[i].h);
+  };
+  HostQueue hq(E->host_threads);  // declared after what its jobs use, so it is joined first
+  // device rows of a block's final pairs; their domain definition is queued
+  // and runs while the engine thread moves on to the next block
+  auto rows_and_queue = [&](Slot& S, BlockOut* B) {
+    B->res.resize(B->finals.size());
+    const auto t0 = std::chrono::steady_clock::now();
+    rows_pass(E, S, P, T, B->finals, [&, B](RowsChunk&& c) {
+      auto ch = std::make_shared<RowsChunk>(std::move(c));
+      hq.push([&, B, ch](int nthr) {
+        // largest pairs first, for an even finish across the workers
+        std::vector<size_t> ord(ch->which.size());
+        std::iota(ord.begin(), ord.end(), (size_t)0);
+        auto cost = [&](size_t q) {
+          const FinalPair& f = B->finals[ch->which[q]];
+          return (double)P->h[f.p].m * (double)T->len[f.t];
+        };
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return cost(a) > cost(b); });
+        parallel_for(ord.size(), nthr, [&](size_t r) {
+          const size_t q = ord[r];
+          define_pair(B, ch->which[q], ch->f.data() + ch->off[q], ch->b.data() + ch->off[q]);
+        });
+      });
+    });
+    rows_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  };
+
+  std::vector<int> unfiltered;
+  for (size_t pi = 0; pi < np; pi++)
+    if (!th[pi].exact) unfiltered.push_back((int)pi);
+  int64_t nfinal = 0;
+  // software pipeline over two slots: block b+1's MSV is queued on the device
+  // before block b's later stages are driven, so it fills the GPU around
+  // their latency-bound tails and around block b's row passes
+  const auto pb = profile_blocks(E, P, T, th);
+  std::vector<BlockRun> runs(pb.size());
+  for (size_t b = 0; b < pb.size(); b++) {
+    runs[b].p0 = pb[b].first;
+    runs[b].p1 = pb[b].second;
+  }
+  if (!runs.empty()) {
+    // other slots' kernels read the thresholds uploaded on slot 0's stream
+    CK(cudaStreamSynchronize(s));
+    cascade_launch(E, E->sl[0], P, T, th, runs[0]);
+  }
+  for (size_t b = 0; b < runs.size(); b++) {
+    Slot& S = E->sl[b % 2];
+    if (b + 1 < runs.size()) cascade_launch(E, E->sl[(b + 1) % 2], P, T, th, runs[b + 1]);
+    outs.push_back(std::make_unique<BlockOut>());
+    BlockOut* B = outs.back().get();
+    while (!cascade_finish(E, S, P, T, th, o, runs[b], B->finals)) cascade_launch(E, S, P, T, th, runs[b]);
+    nfinal += (int64_t)B->finals.size();
+    rows_and_queue(S, B);
+  }
+  if (!unfiltered.empty() && nt > 0) {
+    outs.push_back(std::make_unique<BlockOut>());
+    BlockOut* B = outs.back().get();
+    for (int pi : unfiltered)
+      for (size_t t = 0; t < nt; t++) B->finals.push_back({pi, (int32_t)t, 0.f, 0.f, 0.f, -1});
+    nfinal += (int64_t)B->finals.size();
+    rows_and_queue(E->sl[0], B);
+  }
+  const auto t_dev = std::chrono::steady_clock::now();
+  E->stats.ms[5] = hq.finish();
+  const auto t_end = std::chrono::steady_clock::now();
+  E->stats.pairs_in[4] = nfinal;
   E->stats.pairs_out[4] = n_domain.load();
-  const double rows_total = std::chrono::duration<double, std::milli>(t_end - t_rows).count();
-  E->stats.ms[4] = rows_total - E->host_ms;
-  E->stats.ms[5] = E->host_ms;
   E->stats.pairs_in[5] = n_domain.load();
-  for (const auto& f : finals) E->stats.cells[4] += (double)P->h[f.p].m * T->len[f.t];
+  E->stats.ms[4] = rows_ms;
   E->stats.ms[6] = std::chrono::duration<double, std::milli>(t_end - t_start).count();
+  E->stats.ms[7] = std::chrono::duration<double, std::milli>(t_end - t_dev).count();
   std::vector<std::vector<std::pair<int32_t, HitOut>>> per(np);
-  for (size_t i = 0; i < finals.size(); i++)
-    if (res[i].hit) per[finals[i].p].emplace_back(finals[i].t, std::move(res[i].h));
+  for (auto& B : outs) {
+    for (const auto& f : B->finals) E->stats.cells[4] += (double)P->h[f.p].m * T->len[f.t];
+    for (size_t i = 0; i < B->finals.size(); i++)
+      if (B->res[i].hit) per[B->finals[i].p].emplace_back(B->finals[i].t, std::move(B->res[i].h));
+  }
   return report(P, T, cfg, per, out);
 }
 
@@ -1115,6 +1455,7 @@ int sx_create(const sx_opts* opts, sx_engine** out) {
   e->host_threads = (opts && opts->host_threads > 0) ? opts->host_threads : (int)std::thread::hardware_concurrency();
   e->host_threads = std::max(1, e->host_threads);
   e->batch_bytes = (opts && opts->batch_bytes > 0) ? opts->batch_bytes : (2LL << 30);
+  e->pipeline_blocks = (opts && opts->pipeline_blocks > 0) ? opts->pipeline_blocks : 0;
   try {
     int ndev = 0;
     CK(cudaGetDeviceCount(&ndev));
@@ -1128,13 +1469,7 @@ int sx_create(const sx_opts* opts, sx_engine** out) {
       return fail(SX_EINVAL, std::string("sx_create: device is ") + prop.name + " (sm_" + std::to_string(prop.major) +
                                  std::to_string(prop.minor) + "); this library is built for sm_100a");
     e->num_sms = prop.multiProcessorCount;
-    CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
-    for (auto& ev : e->ev) CK(cudaEventCreate(&ev));
-    for (int a = 0; a < sx_engine::kAux; a++) {
-      CK(cudaStreamCreateWithFlags(&e->aux[a], cudaStreamNonBlocking));
-      CK(cudaEventCreateWithFlags(&e->join_ev[a], cudaEventDisableTiming));
-    }
-    CK(cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming));
+    for (Slot& S : e->sl) S.create();
     (void)kernels();
   } catch (const CudaError& ce) {
     return fail(ce.code, ce.msg);
@@ -1146,15 +1481,7 @@ int sx_create(const sx_opts* opts, sx_engine** out) {
 void sx_destroy(sx_engine* e) {
   if (!e) return;
   cudaSetDevice(e->device);
-  if (e->stream) cudaStreamSynchronize(e->stream);
-  for (auto& ev : e->ev)
-    if (ev) cudaEventDestroy(ev);
-  for (int a = 0; a < sx_engine::kAux; a++) {
-    if (e->aux[a]) cudaStreamDestroy(e->aux[a]);
-    if (e->join_ev[a]) cudaEventDestroy(e->join_ev[a]);
-  }
-  if (e->fork_ev) cudaEventDestroy(e->fork_ev);
-  if (e->stream) cudaStreamDestroy(e->stream);
+  for (Slot& S : e->sl) S.destroy();
   delete e;
 }
 
@@ -1355,7 +1682,7 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
       }
       e->plist.upload(lst.data(), npairs, s);
       e->slots.upload(slot.data(), npairs, s);
-      launch_msv(e, p, t, tiles, e->plist.p, e->scores.p, e->slots.p, nullptr, nullptr, nullptr);
+      launch_msv(e, e->sl[0], e->sl[0].hi, p, t, tiles, e->plist.p, e->scores.p, e->slots.p, nullptr, nullptr, nullptr);
       CK(cudaMemcpyAsync(msv, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
     }
@@ -1406,7 +1733,7 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
     if (forward || backward) {
       std::vector<FinalPair> fp(npairs);
       for (size_t i = 0; i < npairs; i++) fp[i] = {pair_profile[i], pair_target[i], 0.f, 0.f, 0.f, (int32_t)i};
-      rows_pass(e, p, t, fp, [&](size_t i, const float* fr, const float* br) {
+      rows_pass_sync(e, p, t, fp, [&](size_t i, const float* fr, const float* br) {
         const ProfileHost& h = p->h[fp[i].p];
         const int64_t l = t->len[fp[i].t];
         if (l == 0 || h.m == 0) {

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
   float prev[C];
 #pragma unroll
   for (int c = 0; c < C; c++) prev[c] = SX_NEG_INF;
-  float xn = 0.f, xb = 0.f, xj = SX_NEG_INF, xc = SX_NEG_INF, tloop = 0.f, tmove = 0.f, nullsc = 0.f, fin = SX_NEG_INF;
+  float xn = 0.f, xb = 0.f, xj = SX_NEG_INF, tloop = 0.f, tmove = 0.f, nullsc = 0.f, fin = SX_NEG_INF;
   int entry = -1, tgt = 0, L = 0, row = 0, boff = 0;
   const uint8_t* seq = res;
   uint4 rcur = make_uint4(0x18181818u, 0x18181818u, 0x18181818u, 0x18181818u), rnext = rcur;
@@ -150,6 +150,7 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
     if (!done && row >= L) {  // group-uniform: finish the current target, fetch the next
       if (active && j == 0) {
         const int p = tile.p;
+        fin = fadd(fin, tmove);  // xc at row L, then C->T
         if (score_out) score_out[slot ? slot[entry] : entry] = fin;
         if (surv && bits_stat(fin, nullsc) >= s1) {
           PairRec r;
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
         seq = res + toff[tgt];
         const float4 tp = tpar[tgt];
         tloop = tp.x; tmove = tp.y; nullsc = tp.z;
-        xn = 0.f; xb = tmove; xj = SX_NEG_INF; xc = SX_NEG_INF; fin = SX_NEG_INF;
+        xn = 0.f; xb = tmove; xj = SX_NEG_INF; fin = SX_NEG_INF;
 #pragma unroll
         for (int c = 0; c < C; c++) prev[c] = SX_NEG_INF;
         row = 0;
@@ -219,11 +220,14 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
       for (int b = 1; b < C / 8; b += 2) xe = (b + 1 < C / 8) ? fmx3(xe, blk[b], blk[b + 1]) : fmx(xe, blk[b]);
 #pragma unroll
       for (int o = G / 2; o >= 1; o >>= 1) xe = fmx(xe, __shfl_xor_sync(kFull, xe, o, G));
+      // J and C follow the same recurrence from the same start (E->J and E->C
+      // are both ln 1/2, J->J and C->C both tloop), so xc == xj on every row;
+      // and max(xn+t, xj+t) == max(xn, xj)+t because f32 addition rounds
+      // monotonically.  Both rewrites are exact.
       xj = fmx(fadd(xj, tloop), fadd(xe, -kLn2));
-      xc = fmx(fadd(xc, tloop), fadd(xe, -kLn2));
       xn = fadd(xn, tloop);
-      xb = fmx(fadd(xn, tmove), fadd(xj, tmove));
-      if (rem == r + 1) fin = fadd(xc, tmove);
+      xb = fadd(fmx(xn, xj), tmove);
+      if (rem == r + 1) fin = xj;
     }
     row += 4;
     if (row - boff == 16) {
@@ -803,7 +807,7 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
   unsigned next = (blockIdx.x * blockDim.x + threadIdx.x) / G;  // this group's next list position
 
   float mp[C], ip[C], dp[C];
-  float xn = 0.f, xb = 0.f, xj = SX_NEG_INF, xc = SX_NEG_INF, fin = SX_NEG_INF;
+  float xn = 0.f, xb = 0.f, xj = SX_NEG_INF, fin = SX_NEG_INF;
   float lloop = 0.f, lmove = 0.f;
   int M = 0, L = 0, row = 0;
   bool active = false, done = false;
@@ -829,7 +833,7 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
         const float4 xs = xsc[r.t];
         lloop = xs.x;
         lmove = xs.y;
-        xn = 0.f; xb = lmove; xj = SX_NEG_INF; xc = SX_NEG_INF;
+        xn = 0.f; xb = lmove; xj = SX_NEG_INF;
         fin = SX_NEG_INF;
 #pragma unroll
         for (int c = 0; c < C; c++) mp[c] = ip[c] = dp[c] = SX_NEG_INF;
@@ -925,12 +929,12 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
     for (int b = 1; b < C / 8; b++) xe = fmx(xe, blk[b]);
 #pragma unroll
     for (int o = G / 2; o >= 1; o >>= 1) xe = fmx(xe, __shfl_xor_sync(kFull, xe, o, G));
+    // xc == xj and max(xn+t, xj+t) == max(xn, xj)+t, exactly (as in msv_kernel)
     xj = fmx(fadd(xj, lloop), fadd(xe, -kLn2));
-    xc = fmx(fadd(xc, lloop), fadd(xe, -kLn2));
     xn = fadd(xn, lloop);
-    xb = fmx(fadd(xn, lmove), fadd(xj, lmove));
+    xb = fadd(fmx(xn, xj), lmove);
     row++;
-    if (row == L) fin = fadd(xc, lmove);
+    if (row == L) fin = fadd(xj, lmove);
   }
 }
 

@@ -17,7 +17,7 @@ _PP = C.POINTER(C.c_void_p)
 
 
 class SxOpts(C.Structure):
-    _fields_ = [("device", C.c_int32), ("host_threads", C.c_int32), ("flags", C.c_uint32), ("reserved", C.c_int32),
+    _fields_ = [("device", C.c_int32), ("host_threads", C.c_int32), ("flags", C.c_uint32), ("pipeline_blocks", C.c_int32),
                 ("batch_bytes", C.c_int64)]
 
 
@@ -131,9 +131,9 @@ def _ptr(a, t):
 class Engine:
     """One engine per device (sx_create)."""
 
-    def __init__(self, device=0, host_threads=0, plain=False, batch_bytes=0):
+    def __init__(self, device=0, host_threads=0, plain=False, batch_bytes=0, pipeline_blocks=0):
         lib = load_library()
-        o = SxOpts(device, host_threads, SX_FLAG_PLAIN if plain else 0, 0, batch_bytes)
+        o = SxOpts(device, host_threads, SX_FLAG_PLAIN if plain else 0, pipeline_blocks, batch_bytes)
         h = C.c_void_p()
         _check(lib.sx_create(C.byref(o), C.byref(h)))
         self.h = h

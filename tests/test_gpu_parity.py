@@ -205,6 +205,23 @@ def test_plain_engine_same_hits():
         plain.close()
 
 
+def test_pipeline_blocks_same_hits():
+    """Profile blocks whose host domain definition overlaps later blocks'
+    device cascade (pipeline_blocks=3) give the oracle's hits, as one block does."""
+    w = small_config(1, 0.01)
+    seqs = [(w.target_ids[i], "".join("ACDEFGHIKLMNPQRSTVWY"[x] for x in s)) for i, s in enumerate(w.targets)]
+    a = _hits_oracle(w.hmm_text(), seqs, O.make_cfg())
+    for nb in (1, 3):
+        e = sxhmm.Engine(pipeline_blocks=nb)
+        try:
+            _assert_same_hits(a, _hits_gpu(e, w.hmm_text(), seqs, {}))
+            st = e.stats()
+            assert st["pairs_in"][0] == len(w.profiles) * len(seqs)
+            assert st["ms"][5] >= 0 and st["ms"][7] <= st["ms"][6]
+        finally:
+            e.close()
+
+
 def test_forward_error_vs_fp64_logspace(engine):
     """FP32 odds-space Forward with per-row scaling (bit-identical to the
     reference) against an FP64 log-space Forward: within 0.01 bits."""

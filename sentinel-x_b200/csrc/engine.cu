@@ -17,6 +17,7 @@
 // Steps 1-5 run per block of profiles; a block's host domain definition is
 // queued to a background pool and overlaps the device work of later blocks.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -50,6 +51,13 @@ using sxk::Thresholds;
 namespace {
 
 thread_local std::string g_err;
+
+// Names the kernels of one entry-point call for profilers (a no-op unless a
+// tool is attached), e.g. ncu --nvtx --nvtx-include "sx_search/".
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 int fail(int code, const std::string& msg) {
   g_err = msg;
@@ -136,7 +144,7 @@ typedef void (*VitFn)(const PairRec*, const unsigned*, const BinRegion*, int, Pa
                       const int32_t*, const float4*, float, float*);
 typedef void (*VitGFn)(const PairRec*, const unsigned*, const BinRegion*, int, PairRec*, const BinRegion*, unsigned*,
                        unsigned*, const DevProfile*, const Thresholds*, const float4*, const uint8_t*, const int64_t*,
-                       const int32_t*, const float4*, float, float*);
+                       const int32_t*, const float4*, float, float*, unsigned*);
 typedef void (*FwdFn)(const PairRec*, const unsigned*, const BinRegion*, int, PairRec*, const BinRegion*, unsigned*,
                       unsigned*, const DevProfile*, const Thresholds*, const float*, const uint8_t*, const int64_t*,
                       const int32_t*, const float4*, float, float*, const int64_t*);
@@ -243,6 +251,14 @@ int choose_vit_shape(int m) {
   }
   return best;
 }
+// Persistent grid for a lane-group Viterbi launch of `n` pairs: the CTAs that
+// fit on the GPU at once (two per SM for C <= 16, whose registers are capped
+// at 128, one otherwise), fewer if the pairs need fewer groups.
+int vit_blocks(int num_sms, int shape, unsigned n) {
+  const int g = kVitShapes[shape].g, per_sm = kVitShapes[shape].c <= 16 ? 2 : 1;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n * g + 255) / 256, (int64_t)num_sms * per_sm));
+}
+
 int choose_vbin(int m) {
   const int need = (m + 31) / 32;
   for (int b = 0; b < kNumVbins; b++)
@@ -390,6 +406,7 @@ struct Slot {
   DevBuf<BinRegion> bins[4];
   DevBuf<unsigned> counts;  // 4 stages x kMaxBins
   DevBuf<unsigned> overflow;
+  DevBuf<unsigned> cursor;  // kMaxBins pair cursors of the Viterbi launches
   DevBuf<MsvTile> tiles;
   void create() {
     int least = 0, greatest = 0;
@@ -1101,6 +1118,10 @@ void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets*
                                           kSlackBits, nullptr, P->d_prof.p);
     E->stats.kernel_launches++;
   } else {
+    if (si == 1) {
+      S.cursor.alloc(kMaxBins);
+      CK(cudaMemsetAsync(S.cursor.p, 0, sizeof(unsigned) * kMaxBins, S.hi.main));
+    }
     fork_aux(S.hi);
     int lane = 0;
     const int nb = si == 1 ? kNumVitShapes : kNumVbins;
@@ -1118,11 +1139,10 @@ void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets*
         continue;
       }
       if (si == 1) {
-        const int g = kVitShapes[b].g;
-        const int vblocks = (int)std::min<int64_t>(((int64_t)nin[b] * g + 255) / 256, (int64_t)E->num_sms * 16);
+        const int vblocks = vit_blocks(E->num_sms, b, nin[b]);
         K.vitg[b]<<<vblocks, 256, 0, s>>>(S.lists[1].p, cin, S.bins[1].p, b, S.lists[2].p, S.bins[2].p, cout,
                                           S.overflow.p, P->d_prof.p, E->thr.p, P->d_vit.p, T->d_res.p, T->d_off.p,
-                                          T->d_len.p, T->d_xsc.p, kSlackBits, nullptr);
+                                          T->d_len.p, T->d_xsc.p, kSlackBits, nullptr, S.cursor.p);
       } else
         K.fwd[b]<<<blocks, 256, 0, s>>>(S.lists[2].p, cin, S.bins[2].p, b, S.lists[3].p, S.bins[3].p, cout,
                                         S.overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
@@ -1612,6 +1632,7 @@ int sx_search(sx_engine* e, const sx_profiles* p, const sx_targets* t, const sx_
   if (p->eng != e || t->eng != e) return fail(SX_EINVAL, "sx_search: profiles/targets belong to another engine");
   *out = nullptr;
   std::lock_guard<std::mutex> lk(e->mu);
+  NvtxRange nv("sx_search");
   auto h = std::make_unique<sx_hits>();
   try {
     CK(cudaSetDevice(e->device));
@@ -1643,6 +1664,7 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
                    float* backward, float* bias) {
   if (!e || !p || !t || (npairs && (!pair_profile || !pair_target))) return fail(SX_EINVAL, "sx_score_pairs: NULL argument");
   std::lock_guard<std::mutex> lk(e->mu);
+  NvtxRange nv("sx_score_pairs");
   const size_t np = p->h.size(), nt = t->len.size();
   for (size_t i = 0; i < npairs; i++)
     if (pair_profile[i] < 0 || (size_t)pair_profile[i] >= np || pair_target[i] < 0 || (size_t)pair_target[i] >= nt)
@@ -1717,13 +1739,14 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
         CK(cudaStreamSynchronize(s));
       }
       if (viterbi) {
+        e->sl[0].cursor.alloc(kMaxBins);
+        CK(cudaMemsetAsync(e->sl[0].cursor.p, 0, sizeof(unsigned) * kMaxBins, s));
         for (int b = 0; b < kNumVitShapes; b++) {
           if (!cnt[b]) continue;
-          const int g = kVitShapes[b].g;
-          const int blocks = (int)std::min<int64_t>(((int64_t)cnt[b] * g + 255) / 256, (int64_t)e->num_sms * 16);
+          const int blocks = vit_blocks(e->num_sms, b, cnt[b]);
           K.vitg[b]<<<blocks, 256, 0, s>>>(e->lists[0].p, e->counts.p, e->bins[0].p, b, nullptr, nullptr, nullptr,
                                            e->overflow.p, p->d_prof.p, e->thr.p, p->d_vit.p, t->d_res.p, t->d_off.p,
-                                           t->d_len.p, t->d_xsc.p, 0.f, e->scores.p);
+                                           t->d_len.p, t->d_xsc.p, 0.f, e->scores.p, e->sl[0].cursor.p);
         }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(viterbi, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));

@@ -793,7 +793,8 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
     int bin, PairRec* __restrict__ out, const BinRegion* __restrict__ out_bins, unsigned* __restrict__ out_counts,
     unsigned* __restrict__ overflow, const DevProfile* __restrict__ profs, const Thresholds* __restrict__ thr,
     const float4* __restrict__ vimg, const uint8_t* __restrict__ res, const int64_t* __restrict__ toff,
-    const int32_t* __restrict__ tlen, const float4* __restrict__ xsc, float slack, float* __restrict__ score_out) {
+    const int32_t* __restrict__ tlen, const float4* __restrict__ xsc, float slack, float* __restrict__ score_out,
+    unsigned* __restrict__ cursor) {
   static_assert(C % 8 == 0 && (G & (G - 1)) == 0 && G <= 32, "bad Viterbi shape");
   constexpr int NC4 = C / 4;
   constexpr int ROW4 = NC4 * G;
@@ -803,17 +804,18 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
   const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << gl);
   const unsigned n = min(in_counts[bin], in_bins[bin].cap);
   const int64_t base = in_bins[bin].off;
-  const unsigned ngroups = (gridDim.x * blockDim.x) / G;
-  unsigned next = (blockIdx.x * blockDim.x + threadIdx.x) / G;  // this group's next list position
 
   float mp[C], ip[C], dp[C];
   float xn = 0.f, xb = 0.f, xj = SX_NEG_INF, fin = SX_NEG_INF;
   float lloop = 0.f, lmove = 0.f;
-  int M = 0, L = 0, row = 0;
+  int M = 0, L = 0, row = 0, boff = 0;
   bool active = false, done = false;
   PairRec r{};
   const float4* img = vimg;
   const uint8_t* s = res;
+  // residues 16 at a time from 16-byte words, one word fetched ahead (targets
+  // are 16-byte aligned with slack after the last one)
+  uint4 rcur = make_uint4(0x18181818u, 0x18181818u, 0x18181818u, 0x18181818u), rnext = rcur;
   for (;;) {
     if (!done && row >= L) {  // group-uniform: finish the pair, take the next one
       if (active && j == 0) {
@@ -822,9 +824,13 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
         else if (bits_stat(fin, r.filtersc) >= thr[r.p].s2 - slack)
           push_pair(r, profs[r.p].vbin, out, out_bins, out_counts, overflow);
       }
-      if (next < n) {
-        r = in[base + next];
-        next += ngroups;
+      // pairs are handed out in list order, so the groups resident on an SM
+      // work on neighbouring pairs (mostly one profile: its image stays in L1)
+      unsigned e = 0;
+      if (j == 0) e = atomicAdd(cursor + bin, 1u);
+      e = __shfl_sync(gmask, e, gl);
+      if (e < n) {
+        r = in[base + e];
         const DevProfile P = profs[r.p];
         img = vimg + P.vit_off;
         M = P.m;
@@ -838,6 +844,9 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
 #pragma unroll
         for (int c = 0; c < C; c++) mp[c] = ip[c] = dp[c] = SX_NEG_INF;
         row = 0;
+        boff = 0;
+        rcur = __ldg(reinterpret_cast<const uint4*>(s));
+        rnext = __ldg(reinterpret_cast<const uint4*>(s + 16));
         active = true;
       } else {
         active = false;
@@ -846,7 +855,12 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
       }
     }
     if (__all_sync(kFull, done)) break;
-    const int x = (active && row < L) ? __ldg(s + row) : 24;
+    int x = 24;
+    if (active && row < L) {
+      const int q = row - boff;
+      const uint32_t w = (q >> 2) == 0 ? rcur.x : (q >> 2) == 1 ? rcur.y : (q >> 2) == 2 ? rcur.z : rcur.w;
+      x = (w >> (8 * (q & 3))) & 0xff;
+    }
     const bool ins_ok = x != 24;
     const float4* rowx = img + x * ROW4 + j;
     const float4* tr = img + 25 * ROW4 + j;  // transition rows: mm im dm bm mi ii md dd
@@ -935,6 +949,11 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
     xb = fadd(fmx(xn, xj), lmove);
     row++;
     if (row == L) fin = fadd(xj, lmove);
+    if (row - boff == 16) {
+      boff += 16;
+      rcur = rnext;
+      if (active) rnext = __ldg(reinterpret_cast<const uint4*>(s + boff + 16));
+    }
   }
 }
 

@@ -125,9 +125,18 @@ constexpr MsvShape kMsvShapes[] = {
 constexpr int kNumMsvShapes = sizeof(kMsvShapes) / sizeof(kMsvShapes[0]);
 constexpr int kMaxM = 2048;
 // Viterbi lane-group shapes (G lanes per pair, C columns per lane).
-constexpr MsvShape kVitShapes[] = {{1, 8},  {2, 8},   {4, 8},   {8, 8},   {16, 8},  {32, 8},  {1, 16},
-                                   {2, 16}, {4, 16},  {8, 16},  {16, 16}, {32, 16}, {4, 24},  {8, 24},
-                                   {16, 24}, {32, 24}, {32, 32}, {32, 48}, {32, 64}};
+// Viterbi lane-group shapes: G lanes per pair, C columns per lane, rt = the
+// transition rows held in registers for the whole pair (C <= 16).
+struct VitShape {
+  int g, c, rt;
+};
+constexpr VitShape kVitShapes[] = {{1, 8, 0},   {2, 8, 0},   {4, 8, 0},   {8, 8, 0},   {16, 8, 0},  {32, 8, 0},
+                                   {1, 16, 0},  {2, 16, 0},  {4, 16, 0},  {8, 16, 0},  {16, 16, 0}, {32, 16, 0},
+                                   {4, 24, 0},  {8, 24, 0},  {16, 24, 0}, {32, 24, 0}, {32, 32, 0}, {32, 48, 0},
+                                   {32, 64, 0}, {4, 8, 1},   {8, 8, 1},   {16, 8, 1},  {32, 8, 1},  {32, 16, 1}};
+// CTAs of one shape resident per SM: registers are capped at 128 for C <= 16
+// (two 256-thread CTAs) except with 16 register-held transition columns.
+constexpr int vit_ctas_per_sm(const VitShape& v) { return (v.c <= 16 && !(v.rt && v.c > 8)) ? 2 : 1; }
 constexpr int kNumVitShapes = sizeof(kVitShapes) / sizeof(kVitShapes[0]);
 constexpr int kMaxBins = 32;  // survivor lists per stage (vbins or Viterbi shapes)
 static_assert(kNumVitShapes <= kMaxBins, "too many Viterbi shapes");
@@ -169,7 +178,7 @@ struct MsvTable<kNumMsvShapes> {
 template <int I>
 struct VitGTable {
   static void fill(VitGFn* t) {
-    t[I] = sxk::viterbi_g_kernel<kVitShapes[I].g, kVitShapes[I].c>;
+    t[I] = sxk::viterbi_g_kernel<kVitShapes[I].g, kVitShapes[I].c, kVitShapes[I].rt != 0>;
     VitGTable<I + 1>::fill(t);
   }
 };
@@ -241,8 +250,9 @@ int choose_vit_shape(int m) {
   for (int s = 0; s < kNumVitShapes; s++) {
     const int g = kVitShapes[s].g, c = kVitShapes[s].c;
     if (g * c < m) continue;
-    const double per_row = 19.0 * c + 50.0 + 12.0 * std::log2((double)g);
-    const double occ = c <= 16 ? 1.0 : 0.5;  // C <= 16 runs two 256-thread CTAs per SM, wider C one
+    // per-row lane instructions; register-held transitions save the 8 loads per 4 columns
+    const double per_row = (kVitShapes[s].rt ? 9.0 : 19.0) * c + 50.0 + 12.0 * std::log2((double)g);
+    const double occ = vit_ctas_per_sm(kVitShapes[s]) == 2 ? 1.0 : 0.5;
     const double cost = per_row * g / (32.0 * m) / occ;
     if (cost < best_cost * 0.999) {
       best_cost = cost;
@@ -255,7 +265,7 @@ int choose_vit_shape(int m) {
 // fit on the GPU at once (two per SM for C <= 16, whose registers are capped
 // at 128, one otherwise), fewer if the pairs need fewer groups.
 int vit_blocks(int num_sms, int shape, unsigned n) {
-  const int g = kVitShapes[shape].g, per_sm = kVitShapes[shape].c <= 16 ? 2 : 1;
+  const int g = kVitShapes[shape].g, per_sm = vit_ctas_per_sm(kVitShapes[shape]);
   return (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n * g + 255) / 256, (int64_t)num_sms * per_sm));
 }
 

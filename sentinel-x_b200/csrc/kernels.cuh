@@ -787,8 +787,8 @@ namespace sxk {
 // monotone in x).  All groups step rows in lock step; a group that finishes a
 // pair takes the next one, and the score is latched at its last row.
 // ===========================================================================
-template <int G, int C>
-__global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
+template <int G, int C, bool RT>
+__global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) viterbi_g_kernel(
     const PairRec* __restrict__ in, const unsigned* __restrict__ in_counts, const BinRegion* __restrict__ in_bins,
     int bin, PairRec* __restrict__ out, const BinRegion* __restrict__ out_bins, unsigned* __restrict__ out_counts,
     unsigned* __restrict__ overflow, const DevProfile* __restrict__ profs, const Thresholds* __restrict__ thr,
@@ -806,6 +806,9 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
   const int64_t base = in_bins[bin].off;
 
   float mp[C], ip[C], dp[C];
+  // RT: the pair's 8 transition rows for this lane's columns live in
+  // registers (loaded once per pair); otherwise they are re-read every row
+  float4 trr[RT ? 8 : 1][RT ? C / 4 : 1];
   float xn = 0.f, xb = 0.f, xj = SX_NEG_INF, fin = SX_NEG_INF;
   float lloop = 0.f, lmove = 0.f;
   int M = 0, L = 0, row = 0, boff = 0;
@@ -847,6 +850,13 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
         boff = 0;
         rcur = __ldg(reinterpret_cast<const uint4*>(s));
         rnext = __ldg(reinterpret_cast<const uint4*>(s + 16));
+        if constexpr (RT) {
+          const float4* t0 = img + 25 * ROW4 + j;
+#pragma unroll
+          for (int q = 0; q < 8; q++)
+#pragma unroll
+            for (int c4 = 0; c4 < NC4; c4++) trr[q][c4] = __ldg(t0 + (q * NC4 + c4) * G);
+        }
         active = true;
       } else {
         active = false;
@@ -864,6 +874,10 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
     const bool ins_ok = x != 24;
     const float4* rowx = img + x * ROW4 + j;
     const float4* tr = img + 25 * ROW4 + j;  // transition rows: mm im dm bm mi ii md dd
+    auto T = [&](int q, int c4) -> float4 {
+      if constexpr (RT) return trr[q][c4];
+      else return tr[(q * NC4 + c4) * G];
+    };
     // ---- M and I, descending (old values at c and c-1 still in place) ----
     const float mpl0 = __shfl_up_sync(kFull, mp[C - 1], 1, G);
     const float ipl0 = __shfl_up_sync(kFull, ip[C - 1], 1, G);
@@ -871,8 +885,8 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
     const float mpl = j ? mpl0 : SX_NEG_INF, ipl = j ? ipl0 : SX_NEG_INF, dpl = j ? dpl0 : SX_NEG_INF;
 #pragma unroll
     for (int c4 = NC4 - 1; c4 >= 0; c4--) {
-      const float4 tmm = tr[(0 * NC4 + c4) * G], tim = tr[(1 * NC4 + c4) * G], tdm = tr[(2 * NC4 + c4) * G];
-      const float4 tbm = tr[(3 * NC4 + c4) * G], tmi = tr[(4 * NC4 + c4) * G], tii = tr[(5 * NC4 + c4) * G];
+      const float4 tmm = T(0, c4), tim = T(1, c4), tdm = T(2, c4);
+      const float4 tbm = T(3, c4), tmi = T(4, c4), tii = T(5, c4);
       const float4 sc4 = rowx[c4 * G];
 #pragma unroll
       for (int e = 3; e >= 0; e--) {
@@ -891,7 +905,7 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
     float d = SX_NEG_INF;
 #pragma unroll
     for (int c4 = 0; c4 < NC4; c4++) {
-      const float4 tmd = tr[(6 * NC4 + c4) * G], tdd = tr[(7 * NC4 + c4) * G];
+      const float4 tmd = T(6, c4), tdd = T(7, c4);
 #pragma unroll
       for (int e = 0; e < 4; e++) {
         const int c = 4 * c4 + e;
@@ -909,7 +923,7 @@ __global__ void __launch_bounds__(256, C <= 16 ? 2 : 1) viterbi_g_kernel(
 #pragma unroll
       for (int c4 = 0; c4 < NC4; c4++) {
         if (go) {
-          const float4 tdd = tr[(7 * NC4 + c4) * G];
+          const float4 tdd = T(7, c4);
 #pragma unroll
           for (int e = 0; e < 4; e++) {
             const int c = 4 * c4 + e;

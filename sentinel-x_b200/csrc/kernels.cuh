@@ -70,6 +70,17 @@ __device__ __forceinline__ float fmx3(float a, float b, float c) {
   asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
   return d;
 }
+// Maximum over the full warp in one redux: the map f -> bits ^ (sign ? 0x7fffffff : 0)
+// is an order-preserving bijection from non-NaN f32 to int32 and its own inverse,
+// so the result is exactly the f32 maximum (only -0 and +0 are told apart,
+// with -0 below +0, which fmaxf may order either way).
+__device__ __forceinline__ float warp_max_f32(float v) {
+  int k = __float_as_int(v);
+  k ^= (k >> 31) & 0x7fffffff;
+  k = __reduce_max_sync(kFull, k);
+  k ^= (k >> 31) & 0x7fffffff;
+  return __int_as_float(k);
+}
 __device__ __forceinline__ float bits_stat(float sc, float ref) { return __fdiv_rn(__fsub_rn(sc, ref), kLn2); }
 
 __device__ __forceinline__ void push_pair(const PairRec& r, int bin, PairRec* lists, const BinRegion* bins,
@@ -955,8 +966,12 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
     float xe = blk[0];
 #pragma unroll
     for (int b = 1; b < C / 8; b++) xe = fmx(xe, blk[b]);
+    if constexpr (G == 32) {
+      xe = warp_max_f32(xe);
+    } else {
 #pragma unroll
-    for (int o = G / 2; o >= 1; o >>= 1) xe = fmx(xe, __shfl_xor_sync(kFull, xe, o, G));
+      for (int o = G / 2; o >= 1; o >>= 1) xe = fmx(xe, __shfl_xor_sync(kFull, xe, o, G));
+    }
     // xc == xj and max(xn+t, xj+t) == max(xn, xj)+t, exactly (as in msv_kernel)
     xj = fmx(fadd(xj, lloop), fadd(xe, -kLn2));
     xn = fadd(xn, lloop);

@@ -525,8 +525,6 @@ void join_aux(Streams& X) {
     CK(cudaStreamWaitEvent(X.main, X.join_ev[a], 0));
   }
 }
-void fork_aux(sx_engine* E) { fork_aux(E->sl[0].hi); }
-void join_aux(sx_engine* E) { join_aux(E->sl[0].hi); }
 
 // ---- profile packing --------------------------------------------------------
 void pack_profiles(sx_profiles* P) {
@@ -605,8 +603,9 @@ void pack_profiles(sx_profiles* P) {
       row(26, [&](int k) { return t[TIM][k - 1]; }, kNegInf);
       row(27, [&](int k) { return t[TDM][k - 1]; }, kNegInf);
       row(28, [&](int k) { return t[TBM][k]; }, kNegInf);
-      row(29, [&](int k) { return t[TMI][k]; }, kNegInf);
-      row(30, [&](int k) { return t[TII][k]; }, kNegInf);
+      // no insert state at node M: -inf from k = M on keeps I_M.. at -inf
+      row(29, [&](int k) { return k < m ? t[TMI][k] : kNegInf; }, kNegInf);
+      row(30, [&](int k) { return k < m ? t[TII][k] : kNegInf; }, kNegInf);
       row(31, [&](int k) { return t[TMD][k - 1]; }, kNegInf);
       row(32, [&](int k) { return t[TDD][k - 1]; }, kNegInf);
     }

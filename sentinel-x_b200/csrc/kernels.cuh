@@ -816,13 +816,13 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
   const unsigned n = min(in_counts[bin], in_bins[bin].cap);
   const int64_t base = in_bins[bin].off;
 
-  float mp[C], ip[C], dp[C];
+  float mp[C], ip[C], dp[C], pre[C];
   // RT: the pair's 8 transition rows for this lane's columns live in
   // registers (loaded once per pair); otherwise they are re-read every row
   float4 trr[RT ? 8 : 1][RT ? C / 4 : 1];
   float xn = 0.f, xb = 0.f, xj = SX_NEG_INF, fin = SX_NEG_INF;
   float lloop = 0.f, lmove = 0.f;
-  int M = 0, L = 0, row = 0, boff = 0;
+  int L = 0, row = 0, boff = 0;
   bool active = false, done = false;
   PairRec r{};
   const float4* img = vimg;
@@ -847,7 +847,6 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
         r = in[base + e];
         const DevProfile P = profs[r.p];
         img = vimg + P.vit_off;
-        M = P.m;
         L = tlen[r.t];
         s = res + toff[r.t];
         const float4 xs = xsc[r.t];
@@ -856,7 +855,7 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
         xn = 0.f; xb = lmove; xj = SX_NEG_INF;
         fin = SX_NEG_INF;
 #pragma unroll
-        for (int c = 0; c < C; c++) mp[c] = ip[c] = dp[c] = SX_NEG_INF;
+        for (int c = 0; c < C; c++) mp[c] = ip[c] = dp[c] = pre[c] = SX_NEG_INF;
         row = 0;
         boff = 0;
         rcur = __ldg(reinterpret_cast<const uint4*>(s));
@@ -882,37 +881,40 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
       const uint32_t w = (q >> 2) == 0 ? rcur.x : (q >> 2) == 1 ? rcur.y : (q >> 2) == 2 ? rcur.z : rcur.w;
       x = (w >> (8 * (q & 3))) & 0xff;
     }
-    const bool ins_ok = x != 24;
     const float4* rowx = img + x * ROW4 + j;
     const float4* tr = img + 25 * ROW4 + j;  // transition rows: mm im dm bm mi ii md dd
     auto T = [&](int q, int c4) -> float4 {
       if constexpr (RT) return trr[q][c4];
       else return tr[(q * NC4 + c4) * G];
     };
-    // ---- M and I, descending (old values at c and c-1 still in place) ----
-    const float mpl0 = __shfl_up_sync(kFull, mp[C - 1], 1, G);
-    const float ipl0 = __shfl_up_sync(kFull, ip[C - 1], 1, G);
-    const float dpl0 = __shfl_up_sync(kFull, dp[C - 1], 1, G);
-    const float mpl = j ? mpl0 : SX_NEG_INF, ipl = j ? ipl0 : SX_NEG_INF, dpl = j ? dpl0 : SX_NEG_INF;
+    auto pick = [](const float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; };
+    // ip holds this row's I, computed during the previous row; a '*' residue
+    // has no insert emission (rare: a group-uniform branch)
+    if (x == 24) {
 #pragma unroll
-    for (int c4 = NC4 - 1; c4 >= 0; c4--) {
-      const float4 tmm = T(0, c4), tim = T(1, c4), tdm = T(2, c4);
-      const float4 tbm = T(3, c4), tmi = T(4, c4), tii = T(5, c4);
+      for (int c = 0; c < C; c++) ip[c] = SX_NEG_INF;
+    }
+    // ---- M: max(pre, D[k-1] + t_dm, B + t_bm) + msc; pre = max(M[k-1] + t_mm,
+    // I[k-1] + t_im) of the previous row, computed during that row ----
+    const float dpl0 = __shfl_up_sync(kFull, dp[C - 1], 1, G);
+    const float dpl = j ? dpl0 : SX_NEG_INF;
+#pragma unroll
+    for (int c4 = 0; c4 < NC4; c4++) {
+      const float4 tdm = T(2, c4), tbm = T(3, c4);
       const float4 sc4 = rowx[c4 * G];
 #pragma unroll
-      for (int e = 3; e >= 0; e--) {
+      for (int e = 0; e < 4; e++) {
         const int c = 4 * c4 + e;
-        const int k = j * C + c + 1;
-        auto pick = [e](const float4& v) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; };
-        const float mpv = c ? mp[c - 1] : mpl, ipv = c ? ip[c - 1] : ipl, dpv = c ? dp[c - 1] : dpl;
-        const float ni = (k < M && ins_ok) ? fmx(fadd(mp[c], pick(tmi)), fadd(ip[c], pick(tii))) : SX_NEG_INF;
-        const float sc = fmx(fmx(fadd(mpv, pick(tmm)), fadd(ipv, pick(tim))), fmx(fadd(xb, pick(tbm)), fadd(dpv, pick(tdm))));
-        mp[c] = fadd(sc, pick(sc4));
-        ip[c] = ni;
+        const float dpv = c ? dp[c - 1] : dpl;
+        mp[c] = fadd(fmx3(pre[c], fadd(dpv, pick(tdm, e)), fadd(xb, pick(tbm, e))), pick(sc4, e));
       }
     }
-    // ---- D chain, ascending, carry -inf at the lane boundary ----
+    // ---- D chain (ascending, carry -inf at the lane boundary) and, in the
+    // same block so the scheduler can fill the chain's latency, the next
+    // row's pre and I from this row's M and I (I descending, in place) ----
     const float mcl0 = __shfl_up_sync(kFull, mp[C - 1], 1, G);
+    const float ipl0 = __shfl_up_sync(kFull, ip[C - 1], 1, G);
+    const float mcl = j ? mcl0 : SX_NEG_INF, ipl = j ? ipl0 : SX_NEG_INF;
     float d = SX_NEG_INF;
 #pragma unroll
     for (int c4 = 0; c4 < NC4; c4++) {
@@ -920,17 +922,31 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
 #pragma unroll
       for (int e = 0; e < 4; e++) {
         const int c = 4 * c4 + e;
-        auto pick = [e](const float4& v) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; };
-        const float mcv = c ? mp[c - 1] : (j ? mcl0 : SX_NEG_INF);
-        d = fmx(fadd(mcv, pick(tmd)), fadd(d, pick(tdd)));
+        const float mcv = c ? mp[c - 1] : mcl;
+        d = fmx(fadd(mcv, pick(tmd, e)), fadd(d, pick(tdd, e)));
         dp[c] = d;
       }
     }
-    // ---- push carries across the group's lanes (at most G-1 rounds) ----
+#pragma unroll
+    for (int c4 = NC4 - 1; c4 >= 0; c4--) {
+      const float4 tmm = T(0, c4), tim = T(1, c4), tmi = T(4, c4), tii = T(5, c4);
+#pragma unroll
+      for (int e = 3; e >= 0; e--) {
+        const int c = 4 * c4 + e;
+        const float mpv = c ? mp[c - 1] : mcl, ipv = c ? ip[c - 1] : ipl;
+        pre[c] = fmx(fadd(mpv, pick(tmm, e)), fadd(ipv, pick(tim, e)));
+        // I of the next row (t_mi, t_ii are -inf from column M on, so I_M.. stay -inf)
+        ip[c] = fmx(fadd(mp[c], pick(tmi, e)), fadd(ip[c], pick(tii, e)));
+      }
+    }
+    // ---- push carries across the group's lanes (at most G-1 rounds); a
+    // round runs only when some lane's first column improves ----
     for (int it = 0; it < G; it++) {
       const float cin0 = __shfl_up_sync(kFull, dp[C - 1], 1, G);
       float cin = j ? cin0 : SX_NEG_INF;
-      bool go = true, changed = false;
+      const bool need = fadd(cin, pick(T(7, 0), 0)) > dp[0];
+      if (!__any_sync(kFull, need)) break;
+      bool go = true;
 #pragma unroll
       for (int c4 = 0; c4 < NC4; c4++) {
         if (go) {
@@ -938,13 +954,11 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
 #pragma unroll
           for (int e = 0; e < 4; e++) {
             const int c = 4 * c4 + e;
-            const float t = e == 0 ? tdd.x : e == 1 ? tdd.y : e == 2 ? tdd.z : tdd.w;
             if (go) {
-              const float cand = fadd(cin, t);
+              const float cand = fadd(cin, pick(tdd, e));
               if (cand > dp[c]) {
                 dp[c] = cand;
                 cin = cand;
-                changed = true;
               } else {
                 go = false;
               }
@@ -952,7 +966,6 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
           }
         }
       }
-      if (!__any_sync(kFull, changed)) break;
     }
     // ---- row maximum and special states ----
     float blk[C / 8];

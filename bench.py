@@ -62,6 +62,37 @@ def dist_env():
     return ws, rank, local
 
 
+def rank_seed(rank):
+    """Seed of rank `rank`'s profile block: rank 0 searches the single-GPU
+    workload, rank r > 0 a block of the same size drawn with its own seed."""
+    return None if rank == 0 else 1001 + 7919 * rank
+
+
+def reduce_max(vals, dist, device):
+    """Per-value maximum over ranks (identity without a process group)."""
+    if dist is None:
+        return [float(v) for v in vals]
+    import torch
+    t = torch.tensor([float(v) for v in vals], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def reduce_sum(vals, dist, device):
+    """Per-value sum over ranks (identity without a process group)."""
+    if dist is None:
+        return [float(v) for v in vals]
+    import torch
+    t = torch.tensor([float(v) for v in vals], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return [float(v) for v in t.tolist()]
+
+
+def whole_job_gcups(total_cells, ms):
+    """Aggregate throughput: all ranks' DP cells over the slowest rank's time."""
+    return total_cells / (ms / 1e3) / 1e9
+
+
 def workload(scale, rank, scorer=None):
     from sxhmm import synth
     cache = os.environ.get("SXHMM_BENCH_CACHE", "/tmp/sxhmm_bench_cache")
@@ -70,7 +101,7 @@ def workload(scale, rank, scorer=None):
     if os.path.exists(key):
         z = np.load(key, allow_pickle=False)
         return str(z["text"]), z["seq"], z["offs"], z["lens"], int(z["ntarg"])
-    w = synth.make_config(1, scale=scale, seed=None if rank == 0 else 1001 + 7919 * rank, scorer=scorer)
+    w = synth.make_config(1, scale=scale, seed=rank_seed(rank), scorer=scorer)
     if rank:
         # every rank searches the same targets with its own profile block
         w0 = synth.make_config(1, scale=scale)
@@ -319,13 +350,11 @@ def main():
     # steps stays outside), divided by K
     ms_step = sum(times) / len(times) if times else float("nan")
     e2e_ms = sum(e2e_times) / len(e2e_times)
-    if dist is not None:
-        tt = torch.tensor([ms_step, e2e_ms, float(nhits)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_step, e2e_ms = float(tt[0]), float(tt[1])
-    total_cells = cells * ws
-    value = total_cells / (ms_step / 1e3) / 1e9
-    e2e_value = total_cells / (e2e_ms / 1e3) / 1e9
+    # the job takes as long as its slowest rank; its work is every rank's cells
+    ms_step, e2e_ms = reduce_max([ms_step, e2e_ms], dist, "cuda")
+    (total_cells,) = reduce_sum([cells], dist, "cuda")
+    value = whole_job_gcups(total_cells, ms_step)
+    e2e_value = whole_job_gcups(total_cells, e2e_ms)
     # roofline of the dominant kernel (MSV): algorithmic lane-ops per launch / event time
     msv_t = statistics.median(msv_ms) / 1e3
     achieved = MSV_OPS_PER_CELL * statistics.median(msv_cells) / msv_t / 1e12

@@ -269,6 +269,13 @@ int vit_blocks(int num_sms, int shape, unsigned n) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n * g + 255) / 256, (int64_t)num_sms * per_sm));
 }
 
+// Forward/Backward pass kernels run one warp per pair in one-warp CTAs, so a
+// warp that finishes frees its SM slot at once instead of holding it until
+// the longest pair of a larger CTA is done.
+int warp_ctas(int num_sms, unsigned n) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)n, (int64_t)num_sms * 32));
+}
+
 int choose_vbin(int m) {
   const int need = (m + 31) / 32;
   for (int b = 0; b < kNumVbins; b++)
@@ -879,12 +886,12 @@ void rows_pass(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T,
     fork_aux(S.hi);
     for (int b = 0; b < kNumVbins; b++) {
       if (!cnt[b]) continue;
-      const int blocks = (int)std::min<int64_t>((cnt[b] + 7) / 8, (int64_t)E->num_sms * 16);
+      const int blocks = warp_ctas(E->num_sms, cnt[b]);
       cudaStream_t sa = S.hi.aux[(2 * b) % Streams::kAux], sb = S.hi.aux[(2 * b + 1) % Streams::kAux];
-      K.fwd[b]<<<blocks, 256, 0, sa>>>(S.lists[3].p, S.counts.p + 3 * kMaxBins, S.bins[3].p, b, nullptr, nullptr,
+      K.fwd[b]<<<blocks, 32, 0, sa>>>(S.lists[3].p, S.counts.p + 3 * kMaxBins, S.bins[3].p, b, nullptr, nullptr,
                                        nullptr, S.overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p,
                                        T->d_off.p, T->d_len.p, T->d_xsc.p, 0.f, E->rows_f.p, E->row_off.p);
-      K.bwd[b]<<<blocks, 256, 0, sb>>>(S.lists[3].p, S.counts.p + 3 * kMaxBins, S.bins[3].p, b, P->d_prof.p,
+      K.bwd[b]<<<blocks, 32, 0, sb>>>(S.lists[3].p, S.counts.p + 3 * kMaxBins, S.bins[3].p, b, P->d_prof.p,
                                        P->d_vfb.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p, E->rows_b.p,
                                        E->row_off.p);
       E->stats.kernel_launches += 2;
@@ -1136,7 +1143,6 @@ void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets*
     const int nb = si == 1 ? kNumVitShapes : kNumVbins;
     for (int b = 0; b < nb; b++) {
       if (!nin[b]) continue;
-      const int blocks = (int)std::min<int64_t>((nin[b] + 7) / 8, (int64_t)E->num_sms * 16);
       cudaStream_t s = S.hi.aux[lane++ % Streams::kAux];
       if (si == 1 && (E->flags & SX_FLAG_PLAIN)) {
         sxk::plain_viterbi_kernel<<<(unsigned)std::min<int64_t>(nin[b], (int64_t)E->num_sms * 64), sxk::kPlainThreads,
@@ -1153,7 +1159,8 @@ void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets*
                                           S.overflow.p, P->d_prof.p, E->thr.p, P->d_vit.p, T->d_res.p, T->d_off.p,
                                           T->d_len.p, T->d_xsc.p, kSlackBits, nullptr, S.cursor.p);
       } else
-        K.fwd[b]<<<blocks, 256, 0, s>>>(S.lists[2].p, cin, S.bins[2].p, b, S.lists[3].p, S.bins[3].p, cout,
+        K.fwd[b]<<<warp_ctas(E->num_sms, nin[b]), 32, 0, s>>>(S.lists[2].p, cin, S.bins[2].p, b, S.lists[3].p,
+                                                               S.bins[3].p, cout,
                                         S.overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
                                         T->d_len.p, T->d_xsc.p, kSlackBits, nullptr, nullptr);
       E->stats.kernel_launches++;

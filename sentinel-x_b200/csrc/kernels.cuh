@@ -81,6 +81,25 @@ __device__ __forceinline__ float warp_max_f32(float v) {
   k ^= (k >> 31) & 0x7fffffff;
   return __int_as_float(k);
 }
+// Maximum of v[0..N) with the fewest ALU instructions: three-input maxes level
+// by level with the remainders carried up, so at most the last step is a
+// two-input max — floor(N/2) instructions.  Overwrites v; max is exact in any
+// order.
+template <int N>
+__device__ __forceinline__ float max_tree(float* v) {
+  if constexpr (N == 1) {
+    return v[0];
+  } else if constexpr (N == 2) {
+    return fmx(v[0], v[1]);
+  } else {
+    constexpr int T = N / 3, R = N % 3;
+#pragma unroll
+    for (int i = 0; i < T; i++) v[i] = fmx3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+#pragma unroll
+    for (int i = 0; i < R; i++) v[T + i] = v[3 * T + i];
+    return max_tree<T + R>(v);
+  }
+}
 __device__ __forceinline__ float bits_stat(float sc, float ref) { return __fdiv_rn(__fsub_rn(sc, ref), kLn2); }
 
 __device__ __forceinline__ void push_pair(const PairRec& r, int bin, PairRec* lists, const BinRegion* bins,
@@ -105,7 +124,7 @@ __device__ __forceinline__ void push_pair(const PairRec& r, int bin, PairRec* li
 // inside the row loop; the score is latched at row L.
 // ===========================================================================
 template <int G, int C>
-__global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ tiles, const DevProfile* __restrict__ profs,
+__global__ void __launch_bounds__(256, 2) msv_kernel(const MsvTile* __restrict__ tiles, const DevProfile* __restrict__ profs,
                                                   const Thresholds* __restrict__ thr,
                                                   const float4* __restrict__ msv_img, const uint8_t* __restrict__ res,
                                                   const int64_t* __restrict__ toff, const int32_t* __restrict__ tlen,
@@ -201,6 +220,7 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
     const int rem = L - row;  // rows left in the target; the score is latched when it reaches 0
     uint32_t w = q == 0 ? rcur.x : q == 1 ? rcur.y : q == 2 ? rcur.z : rcur.w;
     if (done) w = 0x18181818u;  // '*' rows: all -inf, never read back
+    float xjr[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
       const int x = (w >> (8 * r)) & 0xff;
@@ -219,16 +239,11 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
         prev[c] = fadd(ra, fmx(prev[c - 1], be));
       }
       prev[0] = fadd(rv[0].x, fmx(left, be));
-      // row maximum: a depth-3 tree of 3-input maxes per 8 columns
-      float blk[C / 8];
+      // row maximum: a tree of 3-input maxes over the lane's C columns
+      float tv[C];
 #pragma unroll
-      for (int b = 0; b < C / 8; b++) {
-        const float* v = prev + 8 * b;
-        blk[b] = fmx3(fmx3(v[0], v[1], v[2]), fmx3(v[3], v[4], v[5]), fmx(v[6], v[7]));
-      }
-      float xe = blk[0];
-#pragma unroll
-      for (int b = 1; b < C / 8; b += 2) xe = (b + 1 < C / 8) ? fmx3(xe, blk[b], blk[b + 1]) : fmx(xe, blk[b]);
+      for (int c = 0; c < C; c++) tv[c] = prev[c];
+      float xe = max_tree<C>(tv);
 #pragma unroll
       for (int o = G / 2; o >= 1; o >>= 1) xe = fmx(xe, __shfl_xor_sync(kFull, xe, o, G));
       // J and C follow the same recurrence from the same start (E->J and E->C
@@ -238,8 +253,10 @@ __global__ void __launch_bounds__(256) msv_kernel(const MsvTile* __restrict__ ti
       xj = fmx(fadd(xj, tloop), fadd(xe, -kLn2));
       xn = fadd(xn, tloop);
       xb = fadd(fmx(xn, xj), tmove);
-      if (rem == r + 1) fin = xj;
+      xjr[r] = xj;
     }
+    // the target's last row falls in this block: latch J (= C) at row L
+    if (rem >= 1 && rem <= 4) fin = rem == 1 ? xjr[0] : rem == 2 ? xjr[1] : rem == 3 ? xjr[2] : xjr[3];
     row += 4;
     if (row - boff == 16) {
       boff += 16;
@@ -830,6 +847,20 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
   // residues 16 at a time from 16-byte words, one word fetched ahead (targets
   // are 16-byte aligned with slack after the last one)
   uint4 rcur = make_uint4(0x18181818u, 0x18181818u, 0x18181818u, 0x18181818u), rnext = rcur;
+  float dpl = SX_NEG_INF;  // left lane's D at its last column, previous row
+  int xcur = 24;           // residue of the current row ('*' past the end)
+  float4 scur[NC4];        // its score chunks for this lane's columns
+  auto residue_at = [](const uint4& w4, int q, bool valid) -> int {
+    if (!valid) return 24;
+    const uint32_t w = (q >> 2) == 0 ? w4.x : (q >> 2) == 1 ? w4.y : (q >> 2) == 2 ? w4.z : w4.w;
+    return (w >> (8 * (q & 3))) & 0xff;
+  };
+  auto load_scores = [&](int xr) {
+    const float4* rowx = img + xr * ROW4 + j;
+#pragma unroll
+    for (int c4 = 0; c4 < NC4; c4++) scur[c4] = rowx[c4 * G];
+  };
+  load_scores(24);
   for (;;) {
     if (!done && row >= L) {  // group-uniform: finish the pair, take the next one
       if (active && j == 0) {
@@ -860,6 +891,9 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
         boff = 0;
         rcur = __ldg(reinterpret_cast<const uint4*>(s));
         rnext = __ldg(reinterpret_cast<const uint4*>(s + 16));
+        dpl = SX_NEG_INF;
+        xcur = residue_at(rcur, 0, L > 0);
+        load_scores(xcur);
         if constexpr (RT) {
           const float4* t0 = img + 25 * ROW4 + j;
 #pragma unroll
@@ -875,13 +909,7 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
       }
     }
     if (__all_sync(kFull, done)) break;
-    int x = 24;
-    if (active && row < L) {
-      const int q = row - boff;
-      const uint32_t w = (q >> 2) == 0 ? rcur.x : (q >> 2) == 1 ? rcur.y : (q >> 2) == 2 ? rcur.z : rcur.w;
-      x = (w >> (8 * (q & 3))) & 0xff;
-    }
-    const float4* rowx = img + x * ROW4 + j;
+    const int x = xcur;
     const float4* tr = img + 25 * ROW4 + j;  // transition rows: mm im dm bm mi ii md dd
     auto T = [&](int q, int c4) -> float4 {
       if constexpr (RT) return trr[q][c4];
@@ -895,13 +923,12 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
       for (int c = 0; c < C; c++) ip[c] = SX_NEG_INF;
     }
     // ---- M: max(pre, D[k-1] + t_dm, B + t_bm) + msc; pre = max(M[k-1] + t_mm,
-    // I[k-1] + t_im) of the previous row, computed during that row ----
-    const float dpl0 = __shfl_up_sync(kFull, dp[C - 1], 1, G);
-    const float dpl = j ? dpl0 : SX_NEG_INF;
+    // I[k-1] + t_im) of the previous row, computed during that row; dpl is
+    // the left lane's final D at its last column, from the carry loop ----
 #pragma unroll
     for (int c4 = 0; c4 < NC4; c4++) {
       const float4 tdm = T(2, c4), tbm = T(3, c4);
-      const float4 sc4 = rowx[c4 * G];
+      const float4 sc4 = scur[c4];
 #pragma unroll
       for (int e = 0; e < 4; e++) {
         const int c = 4 * c4 + e;
@@ -941,11 +968,18 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
     }
     // ---- push carries across the group's lanes (at most G-1 rounds); a
     // round runs only when some lane's first column improves ----
+    // Every improving round moves the carries one lane on, so the loop ends
+    // by the vote within G rounds; its last shuffle is the next row's dpl.
+    bool settled = false;
     for (int it = 0; it < G; it++) {
       const float cin0 = __shfl_up_sync(kFull, dp[C - 1], 1, G);
       float cin = j ? cin0 : SX_NEG_INF;
       const bool need = fadd(cin, pick(T(7, 0), 0)) > dp[0];
-      if (!__any_sync(kFull, need)) break;
+      if (!__any_sync(kFull, need)) {
+        dpl = cin;
+        settled = true;
+        break;
+      }
       bool go = true;
 #pragma unroll
       for (int c4 = 0; c4 < NC4; c4++) {
@@ -966,6 +1000,10 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
           }
         }
       }
+    }
+    if (!settled) {
+      const float d0 = __shfl_up_sync(kFull, dp[C - 1], 1, G);
+      dpl = j ? d0 : SX_NEG_INF;
     }
     // ---- row maximum and special states ----
     float blk[C / 8];
@@ -996,6 +1034,9 @@ __global__ void __launch_bounds__(256, (C <= 16 && !(RT && C > 8)) ? 2 : 1) vite
       rcur = rnext;
       if (active) rnext = __ldg(reinterpret_cast<const uint4*>(s + boff + 16));
     }
+    // the next row's residue and score chunks, loaded a row ahead
+    xcur = residue_at(rcur, row - boff, active && row < L);
+    load_scores(xcur);
   }
 }
 

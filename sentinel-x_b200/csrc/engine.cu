@@ -33,6 +33,7 @@
 #include <numeric>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/sxhmm.h"
@@ -494,7 +495,7 @@ struct sx_profiles {
 
 struct sx_targets {
   sx_engine* eng = nullptr;
-  std::vector<std::string> ids;
+  std::vector<std::string> ids;  // caller's names (sx_targets_create); empty for digital sets
   std::vector<uint8_t> dsq;  // packed digital residues, each target 16-byte aligned
   std::vector<int64_t> off;
   std::vector<int32_t> len;
@@ -717,15 +718,22 @@ void pack_targets(sx_targets* T) {
   const size_t n = T->len.size();
   std::vector<float4> tpar(n), xsc(n);
   T->residues = 0;
+  // the length constants depend on L alone: computed once per distinct length
+  std::unordered_map<int64_t, std::pair<float4, float4>> by_len;
   for (size_t i = 0; i < n; i++) {
     const int64_t l = T->len[i];
-    const float lf = (float)l;
-    // MSV length model (src/hmmer/dp.rs:98-100) and the multihit Xsc (model.rs:284-312)
-    const float tloop = std::log(lf / (lf + 3.0f));
-    const float tmove = std::log(3.0f / (lf + 3.0f));
-    tpar[i] = make_float4(tloop, tmove, null1_score(l), 0.0f);
-    const SpecialTr st = special_transitions(l, true);
-    xsc[i] = make_float4(st.loop, st.move, st.ploop, st.pmove);
+    auto it = by_len.find(l);
+    if (it == by_len.end()) {
+      const float lf = (float)l;
+      // MSV length model (src/hmmer/dp.rs:98-100) and the multihit Xsc (model.rs:284-312)
+      const float tloop = std::log(lf / (lf + 3.0f));
+      const float tmove = std::log(3.0f / (lf + 3.0f));
+      const SpecialTr st = special_transitions(l, true);
+      it = by_len.emplace(l, std::make_pair(make_float4(tloop, tmove, null1_score(l), 0.0f),
+                                            make_float4(st.loop, st.move, st.ploop, st.pmove))).first;
+    }
+    tpar[i] = it->second.first;
+    xsc[i] = it->second.second;
     T->residues += (double)l;
   }
   T->order.resize(n);
@@ -1623,14 +1631,24 @@ int sx_targets_create_digital(sx_engine* e, const uint8_t* dsq, const int64_t* o
   std::lock_guard<std::mutex> lk(e->mu);
   auto t = std::make_unique<sx_targets>();
   t->eng = e;
+  size_t total = 64;
   for (size_t i = 0; i < n; i++) {
     if (lens[i] < 0 || offsets[i] < 0 || lens[i] > INT32_MAX) return fail(SX_EINVAL, "sx_targets_create_digital: bad length");
-    for (int64_t q = 0; q < lens[i]; q++)
-      if (dsq[offsets[i] + q] > SYM_STAR)
-        return fail(SX_EINVAL, "sx_targets_create_digital: residue code " + std::to_string(dsq[offsets[i] + q]) +
-                                   " out of range in target " + std::to_string(i));
-    append_target(t.get(), dsq + offsets[i], (size_t)lens[i]);
-    t->ids.push_back(std::to_string(i));
+    total += ((size_t)lens[i] + 15) & ~(size_t)15;
+  }
+  t->dsq.reserve(total);
+  t->off.reserve(n);
+  t->len.reserve(n);
+  for (size_t i = 0; i < n; i++) {
+    const uint8_t* d = dsq + offsets[i];
+    uint8_t hi = 0;  // max code, a loop the compiler vectorises; positions only on failure
+    for (int64_t q = 0; q < lens[i]; q++) hi = std::max(hi, d[q]);
+    if (hi > SYM_STAR)
+      for (int64_t q = 0; q < lens[i]; q++)
+        if (d[q] > SYM_STAR)
+          return fail(SX_EINVAL, "sx_targets_create_digital: residue code " + std::to_string(d[q]) +
+                                     " out of range in target " + std::to_string(i));
+    append_target(t.get(), d, (size_t)lens[i]);
   }
   return finish_targets(e, std::move(t), out);
 }

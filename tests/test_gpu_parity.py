@@ -169,6 +169,28 @@ def test_missing_cutoff_raises_like_reference(engine):
         sxhmm.search_profiles(ps, sxhmm.Targets([("s", "MKA")]), sxhmm.SearchConfig(sxhmm.Cutoff.trusted()), engine)
 
 
+def test_digital_targets_validated(engine):
+    """Digitised targets: a code above 24 ('*') is rejected with its position;
+    the same residues as text and as codes give the same scores."""
+    seqs = [("a", "MKTAYIAKQR"), ("b", "ACDEFGHIKLMNPQRSTVWY*XBZ")]
+    codes = [O.encode(s) for _, s in seqs]
+    lens = np.array([len(c) for c in codes], np.int64)
+    offs = np.array([0, lens[0]], np.int64)
+    flat = np.concatenate(codes).astype(np.uint8)
+    ts = engine.targets_digital(flat, offs, lens)
+    tt = engine.targets([s for _, s in seqs])
+    ps = engine.load_text(tiny_text())
+    pp, pt = np.zeros(2, np.int32), np.arange(2, dtype=np.int32)
+    a = engine.score_pairs(ps, ts, pp, pt)
+    b = engine.score_pairs(ps, tt, pp, pt)
+    for k in a:
+        assert _same(a[k], b[k]), k
+    bad = flat.copy()
+    bad[lens[0] + 3] = 25
+    with pytest.raises(sxhmm.HmmError, match="residue code 25 out of range in target 1"):
+        engine.targets_digital(bad, offs, lens)
+
+
 def test_search_edges(engine):
     text = tiny_text() + small_profiles_text()
     _cmp(engine, text, edge_targets(), cutoff="T", seq=-1e9, dom=-1e9, filters=False)

@@ -27,6 +27,11 @@ import sys
 import threading
 import time
 
+# The engine drives up to 32 streams (two pipeline slots, high- and
+# low-priority sets); give the process that many hardware work queues before
+# anything initialises CUDA, so high-priority stages never queue behind MSV.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "sentinel-x_b200"))
 sys.path.insert(0, ROOT)

@@ -122,7 +122,10 @@ constexpr MsvShape kMsvShapes[] = {
     {4, 8}, {4, 16}, {4, 24}, {4, 32}, {4, 40}, {4, 48}, {4, 56}, {4, 64},
     {8, 8}, {8, 16}, {8, 24}, {8, 32}, {8, 40}, {8, 48}, {8, 56}, {8, 64},
     {16, 8}, {16, 16}, {16, 24}, {16, 32}, {16, 40}, {16, 48}, {16, 56}, {16, 64},
-    {32, 8}, {32, 16}, {32, 24}, {32, 32}, {32, 40}, {32, 48}, {32, 56}, {32, 64}};
+    {32, 8}, {32, 16}, {32, 24}, {32, 32}, {32, 40}, {32, 48}, {32, 56}, {32, 64},
+    // intermediate widths for the common range of M: half the column padding
+    {2, 36}, {2, 44}, {2, 52}, {2, 60}, {4, 36}, {4, 44}, {4, 52}, {4, 60},
+    {8, 36}, {8, 44}, {8, 52}, {8, 60}};
 constexpr int kNumMsvShapes = sizeof(kMsvShapes) / sizeof(kMsvShapes[0]);
 constexpr int kMaxM = 2048;
 // Viterbi lane-group shapes (G lanes per pair, C columns per lane).
@@ -385,12 +388,14 @@ class BlockPool {
 // into it, all of one scheduling priority.
 struct Streams {
   static constexpr int kAux = 8;
+  int naux = kAux;  // auxiliary streams in use
   cudaStream_t main = nullptr;
   cudaStream_t aux[kAux] = {};  // independent launches (shapes, bins) run side by side
   cudaEvent_t fork_ev = nullptr, join_ev[kAux] = {};
-  void create(int priority) {
+  void create(int priority, int n_aux) {
+    naux = std::max(1, std::min(n_aux, kAux));
     CK(cudaStreamCreateWithPriority(&main, cudaStreamNonBlocking, priority));
-    for (int a = 0; a < kAux; a++) {
+    for (int a = 0; a < naux; a++) {
       CK(cudaStreamCreateWithPriority(&aux[a], cudaStreamNonBlocking, priority));
       CK(cudaEventCreateWithFlags(&join_ev[a], cudaEventDisableTiming));
     }
@@ -398,9 +403,9 @@ struct Streams {
   }
   void destroy() {
     if (main) cudaStreamSynchronize(main);
-    for (int a = 0; a < kAux; a++)
+    for (int a = 0; a < naux; a++)
       if (aux[a]) cudaStreamSynchronize(aux[a]);
-    for (int a = 0; a < kAux; a++) {
+    for (int a = 0; a < naux; a++) {
       if (aux[a]) cudaStreamDestroy(aux[a]);
       if (join_ev[a]) cudaEventDestroy(join_ev[a]);
     }
@@ -429,8 +434,11 @@ struct Slot {
   void create() {
     int least = 0, greatest = 0;
     CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    hi.create(greatest);
-    lo.create(least);
+    // 2 slots x (9 + 7) streams = 32, the most hardware work queues a process
+    // can have (CUDA_DEVICE_MAX_CONNECTIONS=32): with fewer queues, streams
+    // share them and a high-priority launch can wait behind queued MSV work
+    hi.create(greatest, 8);
+    lo.create(least, 6);
     for (auto& e : ev) CK(cudaEventCreate(&e));
     CK(cudaEventCreateWithFlags(&msv_done, cudaEventDisableTiming));
   }
@@ -525,10 +533,10 @@ namespace {
 // into the engine stream.
 void fork_aux(Streams& X) {
   CK(cudaEventRecord(X.fork_ev, X.main));
-  for (int a = 0; a < Streams::kAux; a++) CK(cudaStreamWaitEvent(X.aux[a], X.fork_ev, 0));
+  for (int a = 0; a < X.naux; a++) CK(cudaStreamWaitEvent(X.aux[a], X.fork_ev, 0));
 }
 void join_aux(Streams& X) {
-  for (int a = 0; a < Streams::kAux; a++) {
+  for (int a = 0; a < X.naux; a++) {
     CK(cudaEventRecord(X.join_ev[a], X.aux[a]));
     CK(cudaStreamWaitEvent(X.main, X.join_ev[a], 0));
   }
@@ -895,7 +903,7 @@ void rows_pass(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T,
     for (int b = 0; b < kNumVbins; b++) {
       if (!cnt[b]) continue;
       const int blocks = warp_ctas(E->num_sms, cnt[b]);
-      cudaStream_t sa = S.hi.aux[(2 * b) % Streams::kAux], sb = S.hi.aux[(2 * b + 1) % Streams::kAux];
+      cudaStream_t sa = S.hi.aux[(2 * b) % S.hi.naux], sb = S.hi.aux[(2 * b + 1) % S.hi.naux];
       K.fwd[b]<<<blocks, 32, 0, sa>>>(S.lists[3].p, S.counts.p + 3 * kMaxBins, S.bins[3].p, b, nullptr, nullptr,
                                        nullptr, S.overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p,
                                        T->d_off.p, T->d_len.p, T->d_xsc.p, 0.f, E->rows_f.p, E->row_off.p);
@@ -1117,7 +1125,7 @@ void launch_msv(sx_engine* E, Slot& S, Streams& X, const sx_profiles* P, const s
     const size_t rowp = ((size_t)(c / 4) * g + 7) & ~(size_t)7;
     const size_t smem = (size_t)ncopy * (25 * rowp + 8 + g) * sizeof(float4);
     CK(cudaFuncSetAttribute((const void*)K.msv[s], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    K.msv[s]<<<(unsigned)nt, 256, smem, X.aux[lane++ % Streams::kAux]>>>(
+    K.msv[s]<<<(unsigned)nt, 256, smem, X.aux[lane++ % X.naux]>>>(
         S.tiles.p + start[s], P->d_prof.p, E->thr.p, P->d_msv.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_tpar.p,
         d_list, d_scores, d_slot, surv, bins, counts, S.overflow.p);
     E->stats.kernel_launches++;
@@ -1151,7 +1159,7 @@ void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets*
     const int nb = si == 1 ? kNumVitShapes : kNumVbins;
     for (int b = 0; b < nb; b++) {
       if (!nin[b]) continue;
-      cudaStream_t s = S.hi.aux[lane++ % Streams::kAux];
+      cudaStream_t s = S.hi.aux[lane++ % S.hi.naux];
       if (si == 1 && (E->flags & SX_FLAG_PLAIN)) {
         sxk::plain_viterbi_kernel<<<(unsigned)std::min<int64_t>(nin[b], (int64_t)E->num_sms * 64), sxk::kPlainThreads,
                                     0, S.hi.main>>>(S.lists[1].p, cin, S.bins[1].p, b, S.lists[2].p, S.bins[2].p,

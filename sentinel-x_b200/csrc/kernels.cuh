@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(256, 2) msv_kernel(const MsvTile* __restrict__
                                                   float* __restrict__ score_out, const int32_t* __restrict__ slot,
                                                   PairRec* __restrict__ surv, const BinRegion* __restrict__ bins,
                                                   unsigned* __restrict__ counts, unsigned* __restrict__ overflow) {
-  static_assert(C % 8 == 0 && (G & (G - 1)) == 0 && G <= 32, "bad MSV shape");
+  static_assert(C % 4 == 0 && (G & (G - 1)) == 0 && G <= 32, "bad MSV shape");
   constexpr int NC4 = C / 4;
   constexpr int ROW4 = NC4 * G;  // float4 per residue row
   // A quarter-warp (8 lanes) issues one LDS.128 wavefront: with G < 8 it holds

@@ -119,6 +119,29 @@ const char* sx_last_error(void);
 int sx_profiles_load_file(sx_engine* e, const char* path, sx_profiles** out);
 /* Same from an in-memory HMMER3 text; `source` names it in error messages. */
 int sx_profiles_load_text(sx_engine* e, const char* text, size_t len, const char* source, sx_profiles** out);
+/* One profile already configured by the caller, as the plain arrays of
+ * `Profile` (src/hmmer/model.rs:75-113): the input of search_profiles(&[Profile],
+ * ...) (src/hmmer/search.rs:213).  w = m + 1; every array is read during the
+ * call only. */
+typedef struct {
+  const char* name;     /* required */
+  const char* acc;      /* NULL if absent */
+  const char* desc;     /* NULL if absent */
+  int32_t m;            /* model length M, 1..2048 */
+  int32_t has_cutoffs;  /* bit 0 GA, bit 1 TC, bit 2 NC */
+  const float* msc;     /* [25][w] match log-odds msc[x*w+k] (column 0 -inf) */
+  const float* mo;      /* [25][w] match odds */
+  const float* t;       /* [8][w] log transitions of node k: mm mi md im ii dm dd, then bm (B->M_k) */
+  const float* p;       /* [8][w] probability-space copies, same order */
+  const float* compo;   /* [20] composition used by the bias filter */
+  float msv_tbm;        /* ln(2/(M(M+1))) */
+  float ga[2], tc[2], nc[2];
+  int32_t has_stats;    /* bit 0 MSV, bit 1 Viterbi, bit 2 Forward */
+  double msv[2], viterbi[2], forward[2]; /* (mu|tau, lambda) */
+} sx_profile_arrays;
+/* Uploads n configured profiles (replaces nothing on the reference side: its
+ * callers hand `&[Profile]` to search_profiles directly). */
+int sx_profiles_from_arrays(sx_engine* e, const sx_profile_arrays* profiles, size_t n, sx_profiles** out);
 int32_t sx_profiles_count(const sx_profiles* p);
 int sx_profiles_info(const sx_profiles* p, int32_t i, sx_profile_info* out);
 void sx_profiles_free(sx_profiles* p);

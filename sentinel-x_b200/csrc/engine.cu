@@ -1559,6 +1559,54 @@ int sx_profiles_load_text(sx_engine* e, const char* text, size_t len, const char
   return finish_profiles(e, std::move(p), out);
 }
 
+int sx_profiles_from_arrays(sx_engine* e, const sx_profile_arrays* a, size_t n, sx_profiles** out) {
+  if (!e || !out || (n && !a)) return fail(SX_EINVAL, "sx_profiles_from_arrays: NULL argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(e->mu);
+  auto p = std::make_unique<sx_profiles>();
+  p->eng = e;
+  p->h.resize(n);
+  for (size_t i = 0; i < n; i++) {
+    const sx_profile_arrays& s = a[i];
+    const std::string at = "sx_profiles_from_arrays: profile " + std::to_string(i);
+    if (!s.name || !s.msc || !s.mo || !s.t || !s.p || !s.compo) return fail(SX_EINVAL, at + ": NULL field");
+    if (s.m < 1) return fail(SX_EINVAL, at + ": M must be at least 1");
+    ProfileHost& h = p->h[i];
+    const size_t w = (size_t)s.m + 1;
+    h.name = s.name;
+    h.has_acc = s.acc != nullptr;
+    h.has_desc = s.desc != nullptr;
+    if (s.acc) h.acc = s.acc;
+    if (s.desc) h.desc = s.desc;
+    h.m = s.m;
+    h.msc.assign(s.msc, s.msc + NSYM * w);
+    h.mo.assign(s.mo, s.mo + NSYM * w);
+    for (int q = 0; q < NTR; q++) {
+      h.t[q].assign(s.t + q * w, s.t + (q + 1) * w);
+      h.p[q].assign(s.p + q * w, s.p + (q + 1) * w);
+    }
+    h.msv_tbm = s.msv_tbm;
+    std::copy(s.compo, s.compo + NRES, h.compo);
+    h.has_ga = s.has_cutoffs & 1;
+    h.has_tc = (s.has_cutoffs >> 1) & 1;
+    h.has_nc = (s.has_cutoffs >> 2) & 1;
+    for (int q = 0; q < 2; q++) {
+      h.ga[q] = h.has_ga ? s.ga[q] : NAN;
+      h.tc[q] = h.has_tc ? s.tc[q] : NAN;
+      h.nc[q] = h.has_nc ? s.nc[q] : NAN;
+    }
+    h.has_msv = s.has_stats & 1;
+    h.has_vit = (s.has_stats >> 1) & 1;
+    h.has_fwd = (s.has_stats >> 2) & 1;
+    for (int q = 0; q < 2; q++) {
+      h.msv[q] = h.has_msv ? s.msv[q] : NAN;
+      h.vit[q] = h.has_vit ? s.viterbi[q] : NAN;
+      h.fwd[q] = h.has_fwd ? s.forward[q] : NAN;
+    }
+  }
+  return finish_profiles(e, std::move(p), out);
+}
+
 int sx_profiles_load_file(sx_engine* e, const char* path, sx_profiles** out) {
   if (!e || !out || !path) return fail(SX_EINVAL, "sx_profiles_load_file: NULL argument");
   *out = nullptr;

@@ -45,6 +45,15 @@ class SxProfileInfo(C.Structure):
                 ("msv", C.c_double * 2), ("viterbi", C.c_double * 2), ("forward", C.c_double * 2)]
 
 
+class SxProfileArrays(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("acc", C.c_char_p), ("desc", C.c_char_p), ("m", C.c_int32),
+                ("has_cutoffs", C.c_int32), ("msc", C.POINTER(C.c_float)), ("mo", C.POINTER(C.c_float)),
+                ("t", C.POINTER(C.c_float)), ("p", C.POINTER(C.c_float)), ("compo", C.POINTER(C.c_float)),
+                ("msv_tbm", C.c_float), ("ga", C.c_float * 2), ("tc", C.c_float * 2), ("nc", C.c_float * 2),
+                ("has_stats", C.c_int32), ("msv", C.c_double * 2), ("viterbi", C.c_double * 2),
+                ("forward", C.c_double * 2)]
+
+
 class SxSearchStats(C.Structure):
     _fields_ = [("pairs_in", C.c_int64 * 8), ("pairs_out", C.c_int64 * 8), ("cells", C.c_double * 8),
                 ("ms", C.c_double * 8), ("kernel_launches", C.c_int64)]
@@ -63,6 +72,7 @@ SIGNATURES = {
     "sx_last_error": (C.c_char_p, []),
     "sx_profiles_load_file": (C.c_int, [_P, C.c_char_p, _PP]),
     "sx_profiles_load_text": (C.c_int, [_P, C.c_char_p, C.c_size_t, C.c_char_p, _PP]),
+    "sx_profiles_from_arrays": (C.c_int, [_P, C.POINTER(SxProfileArrays), C.c_size_t, _PP]),
     "sx_profiles_count": (C.c_int32, [_P]),
     "sx_profiles_info": (C.c_int, [_P, C.c_int32, C.POINTER(SxProfileInfo)]),
     "sx_profiles_free": (None, [_P]),
@@ -155,6 +165,12 @@ class Engine:
     def load_file(self, path):
         return Profiles(self, path=path)
 
+    def load_arrays(self, profiles):
+        """Configured profiles as arrays (sx_profiles_from_arrays): a list of
+        dicts with name, m, msc [25, M+1], mo [25, M+1], t [8, M+1], p [8, M+1],
+        compo [20], msv_tbm and optional acc, desc, ga/tc/nc, msv/viterbi/forward."""
+        return Profiles(self, arrays=profiles)
+
     def targets(self, seqs, ids=None):
         return TargetSet(self, seqs=seqs, ids=ids)
 
@@ -216,10 +232,41 @@ def _copy(s):
 class Profiles:
     """A configured profile set on the device (sx_profiles)."""
 
-    def __init__(self, engine, text=None, path=None, source="<stream>"):
+    def __init__(self, engine, text=None, path=None, source="<stream>", arrays=None):
         self.engine = engine
         h = C.c_void_p()
-        if path is not None:
+        if arrays is not None:
+            keep, recs = [], (SxProfileArrays * max(1, len(arrays)))()
+            for i, a in enumerate(arrays):
+                m = int(a["m"])
+                buf = {k: np.ascontiguousarray(a[k], np.float32).ravel() for k in ("msc", "mo", "t", "p", "compo")}
+                if buf["msc"].size != 25 * (m + 1) or buf["mo"].size != 25 * (m + 1) or buf["t"].size != 8 * (m + 1) \
+                        or buf["p"].size != 8 * (m + 1) or buf["compo"].size != 20:
+                    raise ValueError(f"profile {i}: array sizes do not match M = {m}")
+                keep.append(buf)
+                r = recs[i]
+                r.name = a["name"].encode()
+                r.acc = a["acc"].encode() if a.get("acc") else None
+                r.desc = a["desc"].encode() if a.get("desc") else None
+                r.m = m
+                for k in ("msc", "mo", "t", "p", "compo"):
+                    setattr(r, k, buf[k].ctypes.data_as(C.POINTER(C.c_float)))
+                r.msv_tbm = float(a["msv_tbm"])
+                r.has_cutoffs = 0
+                for bit, k in enumerate(("ga", "tc", "nc")):
+                    v = a.get(k)
+                    if v is not None and not any(math.isnan(float(x)) for x in v):
+                        r.has_cutoffs |= 1 << bit
+                        setattr(r, k, (C.c_float * 2)(*[float(x) for x in v]))
+                r.has_stats = 0
+                for bit, k in enumerate(("msv", "viterbi", "forward")):
+                    v = a.get(k)
+                    if v is not None and not any(math.isnan(float(x)) for x in v):
+                        r.has_stats |= 1 << bit
+                        setattr(r, k, (C.c_double * 2)(*[float(x) for x in v]))
+            _check(_lib.sx_profiles_from_arrays(engine.h, recs, len(arrays), C.byref(h)))
+            del keep
+        elif path is not None:
             _check(_lib.sx_profiles_load_file(engine.h, os.fsencode(path), C.byref(h)))
         else:
             b = text.encode() if isinstance(text, str) else bytes(text)

@@ -91,8 +91,8 @@ def _hits_oracle(text, seqs, cfg):
     return out
 
 
-def _hits_gpu(engine, text, seqs, cfg_kw):
-    ps = engine.load_text(text)
+def _hits_gpu(engine, text, seqs, cfg_kw, profiles=None):
+    ps = profiles if profiles is not None else engine.load_text(text)
     targets = sxhmm.Targets(seqs)
     cutoff = {"E": sxhmm.Cutoff.evalue(cfg_kw.get("seq", 10.0), cfg_kw.get("dom", 10.0)),
               "T": sxhmm.Cutoff.bits(cfg_kw.get("seq", 0.0), cfg_kw.get("dom", 0.0)),
@@ -167,6 +167,48 @@ def test_missing_cutoff_raises_like_reference(engine):
     ps = engine.load_text(tiny_text())
     with pytest.raises(sxhmm.HmmError, match="TC bit thresholds unavailable on model tiny"):
         sxhmm.search_profiles(ps, sxhmm.Targets([("s", "MKA")]), sxhmm.SearchConfig(sxhmm.Cutoff.trusted()), engine)
+
+
+def _oracle_arrays(text):
+    """Configured profiles as the oracle's arrays (an independent restatement
+    of Hmm::configure), in the form sx_profiles_from_arrays takes."""
+    o = O.Oracle(text=text)
+    out = []
+    for i in range(o.n):
+        a = o.arrays(i)
+        cut, st = o.header(i)
+        out.append(dict(name=o.names[i], m=o.m[i], msc=a["msc"], mo=a["mo"], t=a["t"], p=a["p"], compo=a["compo"],
+                        msv_tbm=a["msv_tbm"], ga=cut[0:2], tc=cut[2:4], nc=cut[4:6], msv=st[0:2], viterbi=st[2:4],
+                        forward=st[4:6]))
+    return out
+
+
+def test_profiles_from_arrays_same_as_text(engine):
+    """Profiles handed over as configured arrays (the input of
+    search_profiles(&[Profile], ...)) search exactly like the same file parsed
+    by the library: same header fields, stage scores and hits."""
+    w = small_config(1, 0.01)
+    text = w.hmm_text()
+    seqs = [(w.target_ids[i], "".join("ACDEFGHIKLMNPQRSTVWY"[x] for x in s)) for i, s in enumerate(w.targets)]
+    pa = engine.load_arrays(_oracle_arrays(text))
+    pt = engine.load_text(text)
+    assert all(i["acc"] is None and i["desc"] is None for i in pa.info)  # none were given
+    for a, b in zip(pa.info, pt.info):
+        for k in ("name", "m", "calibrated"):
+            assert a[k] == b[k], k
+        for k in ("ga", "tc", "nc", "msv", "viterbi", "forward"):
+            assert np.array_equal(np.array(a[k]), np.array(b[k]), equal_nan=True), k
+    ts = engine.targets([s for _, s in seqs[:40]])
+    pp, pt_ = np.meshgrid(np.arange(len(pa)), np.arange(40), indexing="ij")
+    sa = engine.score_pairs(pa, ts, pp.ravel(), pt_.ravel())
+    sb = engine.score_pairs(pt, ts, pp.ravel(), pt_.ravel())
+    for k in sa:
+        assert _same(sa[k], sb[k]), k
+    _assert_same_hits(_hits_gpu(engine, text, seqs, {}, profiles=pt), _hits_gpu(engine, text, seqs, {}, profiles=pa))
+    with pytest.raises(sxhmm.HmmError, match="M must be at least 1"):
+        bad = dict(_oracle_arrays(text)[0], m=0)
+        bad.update(msc=np.zeros(25), mo=np.zeros(25), t=np.zeros(8), p=np.zeros(8))
+        engine.load_arrays([bad])
 
 
 def test_digital_targets_validated(engine):

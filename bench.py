@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain one-pair-per-block kernels")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="also time sx_posterior_grad on the adjoint workload (4,096 pairs, M=300, L>=400)")
     ap.add_argument("--pipeline-blocks", type=int, default=0,
                     help="profile blocks per search (0 = engine default by workload size)")
     return ap.parse_args()
@@ -224,6 +226,47 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def adjoint_run(sxhmm, eng, torch):
+    """sx_posterior_grad (lnZ and the expected counts of every emission and
+    transition, sqrt(L) checkpointed) on the adjoint workload: 16 profiles of
+    M = 300, 256 targets each (L >= 400, 0-3 planted domains)."""
+    from sxhmm import synth
+    cache = os.environ.get("SXHMM_BENCH_CACHE", "/tmp/sxhmm_bench_cache")
+    os.makedirs(cache, exist_ok=True)
+    key = os.path.join(cache, "cfg3.npz")
+    if os.path.exists(key):
+        z = np.load(key, allow_pickle=False)
+        text, seq, offs, lens, pp, pt = str(z["text"]), z["seq"], z["offs"], z["lens"], z["pp"], z["pt"]
+    else:
+        w = synth.make_config(3)
+        text = w.hmm_text()
+        lens = np.array([len(t) for t in w.targets], np.int64)
+        offs = np.zeros(len(lens), np.int64)
+        offs[1:] = np.cumsum(lens)[:-1]
+        seq = np.concatenate(w.targets).astype(np.uint8)
+        pp = np.array([a for a, _ in w.pairs], np.int32)
+        pt = np.array([b for _, b in w.pairs], np.int32)
+        np.savez(key, text=np.array(text), seq=seq, offs=offs, lens=lens, pp=pp, pt=pt)
+    ps = eng.load_text(text, source="adjoint")
+    ts = eng.targets_digital(seq, offs, lens)
+    cells = float(sum(300 * int(lens[t]) for t in pt))
+    eng.posterior_grad(ps, ts, pp, pt, 300)  # warm-up
+    ms = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.posterior_grad(ps, ts, pp, pt, 300)
+        torch.cuda.synchronize()
+        ms.append((time.perf_counter() - t0) * 1e3)
+    ps.close()
+    ts.close()
+    t = statistics.median(ms)
+    return {"pairs": int(len(pp)), "cells": cells, "ms": round(t, 1), "gcups": round(cells / (t / 1e3) / 1e9, 1),
+            "what": "lnZ + gradients w.r.t. all match/insert emission and transition scores per pair "
+                    "(Forward with sqrt(L) checkpoints, Backward with segment recomputation); host arrays "
+                    "out, copies included"}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
@@ -323,6 +366,10 @@ def main():
         rst = reng.stats()
         msv_ms.append(rst["ms"][0])
         msv_cells.append(rst["cells"][0])
+    # stage GCUPS (cells entering a stage / its device time), single-block search
+    stage_gcups = {k: round(rst["cells"][i] / (rst["ms"][i] / 1e3) / 1e9, 1) if rst["ms"][i] > 0 else None
+                   for k, i in (("msv", 0), ("viterbi", 2), ("forward", 3), ("fwd_bwd_rows", 4))}
+    stage_cells = {k: rst["cells"][i] for k, i in (("msv", 0), ("viterbi", 2), ("forward", 3), ("fwd_bwd_rows", 4))}
     rps.close()
     rts.close()
     reng.close()
@@ -388,12 +435,15 @@ def main():
                          "single_block_ms_per_step": round(max(single_ms), 3)},
             "stage_ms": {k: round(v / max(1, args.steps), 3) for k, v in zip(STAGES, stage_ms)},
             "stage_pairs_in": dict(zip(["msv", "bias", "viterbi", "forward", "rows", "host_domains"], stage_pairs or [])),
+            "stage_gcups": stage_gcups, "stage_cells": stage_cells,
             "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps_ms": [round(x, 1) for x in e2e_times],
                     "target_upload_ms": [round(x, 1) for x in e2e_upload],
                     "stage_ms_per_step": e2e_stage, "search_close_ms": e2e_parts},
             "steps_ms": [round(x, 1) for x in times],
             "gpu_launches": int(launches), "clocks": clocks}
+    if args.adjoint:
+        line["adjoint"] = adjoint_run(sxhmm, eng, torch)
     if plain is not None:
         line["plain"] = plain
         line["batched_over_plain"] = plain["ms_per_step"] / ms_step

@@ -430,6 +430,7 @@ struct Slot {
   DevBuf<unsigned> counts;  // 4 stages x kMaxBins
   DevBuf<unsigned> overflow;
   DevBuf<unsigned> cursor;  // kMaxBins pair cursors of the Viterbi launches
+  DevBuf<double> cells;     // DP cells entering each stage (stats)
   DevBuf<MsvTile> tiles;
   void create() {
     int least = 0, greatest = 0;
@@ -1274,6 +1275,8 @@ void cascade_launch(sx_engine* E, Slot& S, const sx_profiles* P, const sx_target
   }
   CK(cudaMemsetAsync(S.counts.p, 0, sizeof(unsigned) * 4 * kMaxBins, s));
   CK(cudaMemsetAsync(S.overflow.p, 0, sizeof(unsigned), s));
+  S.cells.alloc(4);
+  CK(cudaMemsetAsync(S.cells.p, 0, sizeof(double) * 4, s));
   // stage 0: MSV over all pairs of the block's filtered profiles
   CK(cudaEventRecord(S.ev[0], s));
   if (E->flags & SX_FLAG_PLAIN) {
@@ -1313,11 +1316,25 @@ bool cascade_finish(sx_engine* E, Slot& S, const sx_profiles* P, const sx_target
     for (int b = 0; b < kMaxBins; b++) nin[b] = std::min(cnt[si * kMaxBins + b], R.L[si].reg[b].cap);
     CK(cudaEventRecord(S.ev[2 + si], s));
     launch_stage(E, S, P, T, si, nin);
+    if (si >= 1) {  // cells entering Viterbi (si = 1) and the Forward pre-screen (si = 2), for the stats
+      unsigned mx = 0;
+      for (int b = 0; b < kMaxBins; b++) mx = std::max(mx, nin[b]);
+      if (mx) {
+        dim3 grid((unsigned)std::min<int64_t>((mx + 255) / 256, (int64_t)E->num_sms * 4), kMaxBins);
+        sxk::stage_cells_kernel<<<grid, 256, 0, S.hi.aux[0]>>>(S.lists[si].p, S.counts.p + si * kMaxBins,
+                                                                S.bins[si].p, P->d_prof.p, T->d_len.p,
+                                                                S.cells.p + si);
+        E->stats.kernel_launches++;
+      }
+    }
   }
   CK(cudaEventRecord(S.ev[5], s));
   unsigned ovf = 0;
+  double scells[4] = {0, 0, 0, 0};
+  join_aux(S.hi);  // the cell counts run on an auxiliary stream
   CK(cudaMemcpyAsync(cnt.data(), S.counts.p, sizeof(unsigned) * 4 * kMaxBins, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&ovf, S.overflow.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(scells, S.cells.p, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (ovf && R.attempt < kListAttempts - 1) {  // a survivor list was too small
     R.attempt++;
@@ -1334,6 +1351,8 @@ bool cascade_finish(sx_engine* E, Slot& S, const sx_profiles* P, const sx_target
     E->stats.pairs_out[si] += c;
     if (si < 3) E->stats.pairs_in[si + 1] += c;
   }
+  E->stats.cells[2] += scells[1];
+  E->stats.cells[3] += scells[2];
   E->stats.ms[0] += elapsed_ms(S.ev[0], S.ev[1]);
   E->stats.ms[1] += elapsed_ms(S.ev[2], S.ev[3]);
   E->stats.ms[2] += elapsed_ms(S.ev[3], S.ev[4]);

@@ -317,6 +317,26 @@ __global__ void __launch_bounds__(256) bias_kernel(const PairRec* __restrict__ i
   }
 }
 
+// DP cells (sum of M * L) of the pairs in the per-bin lists (grid.y = bin):
+// the work a stage receives, for its GCUPS.  Double atomics per warp; the
+// order of the additions (and so the last bits) may vary between runs.
+__global__ void __launch_bounds__(256) stage_cells_kernel(const PairRec* __restrict__ lists,
+                                                          const unsigned* __restrict__ counts,
+                                                          const BinRegion* __restrict__ bins,
+                                                          const DevProfile* __restrict__ profs,
+                                                          const int32_t* __restrict__ tlen, double* __restrict__ out) {
+  const int b = blockIdx.y;
+  const unsigned n = min(counts[b], bins[b].cap);
+  double acc = 0.0;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const PairRec r = lists[bins[b].off + i];
+    acc += (double)profs[r.p].m * (double)tlen[r.t];
+  }
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc != 0.0) atomicAdd(out, acc);
+}
+
 // Lane-chunked access to the warp-chunked profile image: column k = lane*VC + c + 1.
 template <int VC>
 struct Img {

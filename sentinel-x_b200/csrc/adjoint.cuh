@@ -29,7 +29,7 @@ struct AdjPair {
   int64_t seg_off;  // float offset: (S+1) rows x 3 x 32*VC
   int64_t sp_off;   // float offset: (L+1) x 6 scaled specials (xn xb xe xj xc scale)
   int64_t ls_off;   // double offset: (L+1) cumulative Forward ln scale
-  int64_t out_off;  // float offset of this pair's outputs: d_msc[25][M+1], d_isc[25][M+1], d_tr[8][M+1]
+  int64_t out_off;  // float offset in the output buffer: d_msc[25][M+1], d_isc[25][M+1], d_tr[8][M+1]
 };
 
 // One Forward row (dp.rs:254-296) for a warp: updates (mp, ip, dp) in place to

@@ -484,7 +484,7 @@ struct sx_engine {
   DevBuf<float> scores;
   DevBuf<int32_t> slots, plist;
   DevBuf<sxk::AdjPair> adj_pairs;
-  DevBuf<float> adj_f;
+  DevBuf<float> adj_f, adj_out;
   DevBuf<double> adj_d, adj_lnz;
 };
 
@@ -1906,7 +1906,6 @@ int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, c
     const int vb = p->dp[pair_profile[0]].vbin, VC = kVcBins[vb];
     const auto& K = kernels();
     const int64_t budget = std::max<int64_t>(e->batch_bytes, 64LL << 20);
-    std::vector<float> host_out;
     size_t i0 = 0;
     while (i0 < npairs) {
       // chunk: scratch floats per pair ~ (L/S + S + 2) * 3 * 32 * VC + 6 (L+1) + out, doubles (L+1)
@@ -1917,8 +1916,9 @@ int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, c
         const int64_t L = t->len[pair_target[i1]];
         const int S = std::max<int>(1, (int)std::ceil(std::sqrt((double)std::max<int64_t>(L, 1))));
         const int64_t rowf = 3LL * 32 * VC;
-        const int64_t need_f = (L / S + 1) * rowf + (S + 1) * rowf + 6 * (L + 1) + (int64_t)out_per;
-        if (i1 > i0 && (fo + need_f) * 4 + (dd + L + 1) * 8 > budget) break;
+        const int64_t need_f = (L / S + 1) * rowf + (S + 1) * rowf + 6 * (L + 1);
+        if (i1 > i0 && (fo + need_f + (int64_t)(i1 - i0 + 1) * (int64_t)out_per) * 4 + (dd + L + 1) * 8 > budget)
+          break;
         sxk::AdjPair a{};
         a.p = pair_profile[i1];
         a.t = pair_target[i1];
@@ -1926,9 +1926,9 @@ int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, c
         a.ck_off = fo;
         a.seg_off = a.ck_off + (L / S + 1) * rowf;
         a.sp_off = a.seg_off + (S + 1) * rowf;
-        a.out_off = a.sp_off + 6 * (L + 1);
+        a.out_off = (int64_t)(i1 - i0) * (int64_t)out_per;  // outputs packed per pair in their own buffer
         a.ls_off = dd;
-        fo = a.out_off + (int64_t)out_per;
+        fo = a.sp_off + 6 * (L + 1);
         dd += L + 1;
         ap.push_back(a);
         i1++;
@@ -1936,27 +1936,26 @@ int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, c
       const int n = (int)ap.size();
       e->adj_pairs.upload(ap.data(), ap.size(), s);
       e->adj_f.alloc((size_t)fo);
+      e->adj_out.alloc((size_t)n * out_per);
       e->adj_d.alloc((size_t)std::max<int64_t>(dd, 1));
       e->adj_lnz.alloc((size_t)n);
-      for (const auto& a : ap)
-        CK(cudaMemsetAsync(e->adj_f.p + a.out_off, 0, sizeof(float) * out_per, s));
+      CK(cudaMemsetAsync(e->adj_out.p, 0, sizeof(float) * out_per * (size_t)n, s));
       const int blocks = std::max(1, std::min((n + 3) / 4, e->num_sms * 32));
       K.adjf[vb]<<<blocks, 128, 0, s>>>(e->adj_pairs.p, n, p->d_prof.p, p->d_vfb.p, t->d_res.p, t->d_off.p,
                                         t->d_len.p, t->d_xsc.p, e->adj_f.p, e->adj_d.p, e->adj_lnz.p);
       K.adjb[vb]<<<blocks, 128, 0, s>>>(e->adj_pairs.p, n, p->d_prof.p, p->d_vfb.p, t->d_res.p, t->d_off.p,
-                                        t->d_len.p, t->d_xsc.p, e->adj_f.p, e->adj_d.p, e->adj_lnz.p, e->adj_f.p);
+                                        t->d_len.p, t->d_xsc.p, e->adj_f.p, e->adj_d.p, e->adj_lnz.p, e->adj_out.p);
       CK(cudaGetLastError());
-      host_out.resize((size_t)fo);
-      CK(cudaMemcpyAsync(host_out.data(), e->adj_f.p, sizeof(float) * (size_t)fo, cudaMemcpyDeviceToHost, s));
+      // scatter the packed [25W | 25W | 8W] outputs straight into the caller's three arrays
+      const size_t sp = sizeof(float) * out_per;
+      CK(cudaMemcpy2DAsync(d_msc + i0 * 25 * W, sizeof(float) * 25 * W, e->adj_out.p, sp, sizeof(float) * 25 * W,
+                           (size_t)n, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpy2DAsync(d_isc + i0 * 25 * W, sizeof(float) * 25 * W, e->adj_out.p + 25 * W, sp,
+                           sizeof(float) * 25 * W, (size_t)n, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpy2DAsync(d_trans + i0 * 8 * W, sizeof(float) * 8 * W, e->adj_out.p + 50 * W, sp,
+                           sizeof(float) * 8 * W, (size_t)n, cudaMemcpyDeviceToHost, s));
       CK(cudaMemcpyAsync(lnz + i0, e->adj_lnz.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
-      for (int q = 0; q < n; q++) {
-        const float* src = host_out.data() + ap[q].out_off;
-        const size_t i = i0 + (size_t)q;
-        memcpy(d_msc + i * 25 * W, src, sizeof(float) * 25 * W);
-        memcpy(d_isc + i * 25 * W, src + 25 * W, sizeof(float) * 25 * W);
-        memcpy(d_trans + i * 8 * W, src + 50 * W, sizeof(float) * 8 * W);
-      }
       i0 = i1;
     }
   } catch (const CudaError& ce) {

@@ -142,6 +142,12 @@ typedef struct {
 /* Uploads n configured profiles (replaces nothing on the reference side: its
  * callers hand `&[Profile]` to search_profiles directly). */
 int sx_profiles_from_arrays(sx_engine* e, const sx_profile_arrays* profiles, size_t n, sx_profiles** out);
+/* A binary cache of configured profiles: sx_profiles_save writes the set in
+ * the library's own format (little-endian, versioned, checksummed) and
+ * sx_profiles_load_binary reads it back without parsing or configuring, for
+ * large libraries such as Pfam-A.  No counterpart in the reference. */
+int sx_profiles_save(const sx_profiles* p, const char* path);
+int sx_profiles_load_binary(sx_engine* e, const char* path, sx_profiles** out);
 int32_t sx_profiles_count(const sx_profiles* p);
 int sx_profiles_info(const sx_profiles* p, int32_t i, sx_profile_info* out);
 void sx_profiles_free(sx_profiles* p);
@@ -164,6 +170,14 @@ void sx_targets_free(sx_targets* t);
  * posterior domain definition, envelope rescoring, null2 and reporting.  Hits
  * come out in profile order, then target order, like the reference. */
 int sx_search(sx_engine* e, const sx_profiles* p, const sx_targets* t, const sx_search_cfg* cfg, sx_hits** out);
+/* Batched sx_search for callers that issue many small searches over the same
+ * targets (BUSCO: one single-profile search per file, src/busco/mod.rs:297-304;
+ * CheckV: one search per HMM file, src/checkv/mod.rs:370-371).  The n profile
+ * sets run as one device search; out[i] receives exactly the hits
+ * sx_search(e, sets[i], t, cfg, ...) returns (profile_index relative to set i).
+ * Fails, with out[] all NULL, if sx_search would fail for any set. */
+int sx_search_many(sx_engine* e, const sx_profiles* const* sets, size_t n, const sx_targets* t,
+                   const sx_search_cfg* cfg, sx_hits** out);
 size_t sx_hits_count(const sx_hits* h);
 const sx_hit* sx_hits_array(const sx_hits* h);
 size_t sx_hits_domain_count(const sx_hits* h);

@@ -1638,6 +1638,25 @@ int sx_profiles_load_file(sx_engine* e, const char* path, sx_profiles** out) {
   return finish_profiles(e, std::move(p), out);
 }
 
+int sx_profiles_save(const sx_profiles* p, const char* path) {
+  if (!p || !path) return fail(SX_EINVAL, "sx_profiles_save: NULL argument");
+  std::string err;
+  if (!save_profiles_binary(p->h, path, err)) return fail(SX_EIO, "sx_profiles_save: " + err);
+  return SX_OK;
+}
+
+int sx_profiles_load_binary(sx_engine* e, const char* path, sx_profiles** out) {
+  if (!e || !out || !path) return fail(SX_EINVAL, "sx_profiles_load_binary: NULL argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(e->mu);
+  auto p = std::make_unique<sx_profiles>();
+  p->eng = e;
+  std::string err;
+  bool io = false;
+  if (!load_profiles_binary(path, p->h, err, io)) return fail(io ? SX_EIO : SX_EINVAL, "sx_profiles_load_binary: " + err);
+  return finish_profiles(e, std::move(p), out);
+}
+
 int32_t sx_profiles_count(const sx_profiles* p) { return p ? (int32_t)p->h.size() : 0; }
 
 int sx_profiles_info(const sx_profiles* p, int32_t i, sx_profile_info* out) {
@@ -1753,6 +1772,62 @@ int sx_search(sx_engine* e, const sx_profiles* p, const sx_targets* t, const sx_
     return fail(SX_ENOMEM, "sx_search: host allocation failed");
   }
   *out = h.release();
+  return SX_OK;
+}
+
+int sx_search_many(sx_engine* e, const sx_profiles* const* sets, size_t n, const sx_targets* t,
+                   const sx_search_cfg* cfg, sx_hits** out) {
+  if (!e || !t || !cfg || !out || (n && !sets)) return fail(SX_EINVAL, "sx_search_many: NULL argument");
+  for (size_t i = 0; i < n; i++) out[i] = nullptr;
+  if (t->eng != e) return fail(SX_EINVAL, "sx_search_many: targets belong to another engine");
+  for (size_t i = 0; i < n; i++)
+    if (!sets[i] || sets[i]->eng != e)
+      return fail(SX_EINVAL, "sx_search_many: profile set " + std::to_string(i) + " is NULL or of another engine");
+  std::lock_guard<std::mutex> lk(e->mu);
+  // the first set sx_search would reject decides the error
+  for (size_t i = 0; i < n; i++) {
+    const int rc = check_cutoffs(sets[i], cfg->cutoff_kind);
+    if (rc) return rc;
+  }
+  // One combined set.  Search and report treat every profile on its own
+  // (per-profile thresholds, E-values over the same targets, per-profile
+  // domain Z), so slicing the combined hits by profile range is exact.
+  std::vector<size_t> first(n + 1, 0);
+  auto all = std::make_unique<sx_profiles>();
+  all->eng = e;
+  for (size_t i = 0; i < n; i++) {
+    first[i] = all->h.size();
+    all->h.insert(all->h.end(), sets[i]->h.begin(), sets[i]->h.end());
+  }
+  first[n] = all->h.size();
+  std::vector<std::unique_ptr<sx_hits>> parts(n);
+  try {
+    CK(cudaSetDevice(e->device));
+    sx_hits hits;
+    if (!all->h.empty()) {
+      pack_profiles(all.get());
+      const int rc = run_search(e, all.get(), t, cfg, &hits);
+      if (rc) return rc;
+    }
+    size_t q = 0;
+    for (size_t i = 0; i < n; i++) {
+      parts[i] = std::make_unique<sx_hits>();
+      sx_hits& part = *parts[i];
+      while (q < hits.hits.size() && (size_t)hits.hits[q].profile_index < first[i + 1]) {
+        sx_hit hh = hits.hits[q++];
+        const sx_domain* d = hits.doms.data() + hh.domain_offset;
+        hh.profile_index -= (int32_t)first[i];
+        hh.domain_offset = (int32_t)part.doms.size();
+        part.doms.insert(part.doms.end(), d, d + hh.ndomains);
+        part.hits.push_back(hh);
+      }
+    }
+  } catch (const CudaError& ce) {
+    return fail(ce.code, ce.msg);
+  } catch (const std::bad_alloc&) {
+    return fail(SX_ENOMEM, "sx_search_many: host allocation failed");
+  }
+  for (size_t i = 0; i < n; i++) out[i] = parts[i].release();
   return SX_OK;
 }
 

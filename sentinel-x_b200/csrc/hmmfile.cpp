@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "internal.hpp"
 
@@ -507,5 +508,192 @@ double gumbel_survival(double x, double mu, double lambda) {
 }
 
 double exp_tail_logsurv(double x, double tau, double lambda) { return x < tau ? 0.0 : -lambda * (x - tau); }
+
+// ---- binary cache of configured profiles ---------------------------------------
+// Layout (little-endian): "SXPROF01", u32 version = 1, u32 count, then per
+// profile: string name, u8 has_acc, string acc, u8 has_desc, string desc,
+// i32 M, u8 flags (GA TC NC MSV VIT FWD), f32 ga[2] tc[2] nc[2],
+// f64 msv[2] vit[2] fwd[2], f32 msv_tbm, f32 compo[20], f32 msc[25(M+1)],
+// mo[25(M+1)], t[8(M+1)], p[8(M+1)]; finally u64 FNV-1a of everything after
+// the magic.  Strings are u32 length + bytes.
+namespace {
+
+constexpr char kBinMagic[8] = {'S', 'X', 'P', 'R', 'O', 'F', '0', '1'};
+constexpr uint32_t kBinVersion = 1;
+
+uint64_t fnv1a(const uint8_t* p, size_t n) {
+  uint64_t h = 1469598103934665603ull;
+  for (size_t i = 0; i < n; i++) {
+    h ^= p[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+class ByteWriter {
+ public:
+  template <typename T>
+  void put(const T& v) { raw(&v, sizeof v); }
+  void raw(const void* p, size_t n) {
+    const uint8_t* b = static_cast<const uint8_t*>(p);
+    buf.insert(buf.end(), b, b + n);
+  }
+  void str(const std::string& s) {
+    put<uint32_t>((uint32_t)s.size());
+    raw(s.data(), s.size());
+  }
+  void floats(const std::vector<float>& v) { raw(v.data(), sizeof(float) * v.size()); }
+  std::vector<uint8_t> buf;
+};
+
+class ByteReader {
+ public:
+  ByteReader(const uint8_t* p, size_t n) : p_(p), n_(n) {}
+  template <typename T>
+  bool get(T& v) { return raw(&v, sizeof v); }
+  bool raw(void* out, size_t n) {
+    if (n > n_ - o_) return false;
+    std::memcpy(out, p_ + o_, n);
+    o_ += n;
+    return true;
+  }
+  bool str(std::string& s) {
+    uint32_t n = 0;
+    if (!get(n) || n > n_ - o_) return false;
+    s.assign(reinterpret_cast<const char*>(p_ + o_), n);
+    o_ += n;
+    return true;
+  }
+  bool floats(std::vector<float>& v, size_t n) {
+    if (n > (n_ - o_) / sizeof(float)) return false;
+    v.resize(n);
+    return raw(v.data(), sizeof(float) * n);
+  }
+  size_t left() const { return n_ - o_; }
+
+ private:
+  const uint8_t* p_;
+  size_t n_, o_ = 0;
+};
+
+}  // namespace
+
+bool save_profiles_binary(const std::vector<ProfileHost>& in, const std::string& path, std::string& err) {
+  ByteWriter w;
+  w.put<uint32_t>(kBinVersion);
+  w.put<uint32_t>((uint32_t)in.size());
+  for (const ProfileHost& h : in) {
+    w.str(h.name);
+    w.put<uint8_t>(h.has_acc);
+    w.str(h.acc);
+    w.put<uint8_t>(h.has_desc);
+    w.str(h.desc);
+    w.put<int32_t>(h.m);
+    const uint8_t flags = (uint8_t)(h.has_ga | h.has_tc << 1 | h.has_nc << 2 | h.has_msv << 3 | h.has_vit << 4 |
+                                    h.has_fwd << 5);
+    w.put(flags);
+    w.raw(h.ga, sizeof h.ga);
+    w.raw(h.tc, sizeof h.tc);
+    w.raw(h.nc, sizeof h.nc);
+    w.raw(h.msv, sizeof h.msv);
+    w.raw(h.vit, sizeof h.vit);
+    w.raw(h.fwd, sizeof h.fwd);
+    w.put(h.msv_tbm);
+    w.raw(h.compo, sizeof h.compo);
+    w.floats(h.msc);
+    w.floats(h.mo);
+    for (int q = 0; q < NTR; q++) w.floats(h.t[q]);
+    for (int q = 0; q < NTR; q++) w.floats(h.p[q]);
+  }
+  const uint64_t sum = fnv1a(w.buf.data(), w.buf.size());
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) {
+    err = path + ": " + std::strerror(errno);
+    return false;
+  }
+  bool ok = std::fwrite(kBinMagic, 1, sizeof kBinMagic, f) == sizeof kBinMagic;
+  ok = ok && std::fwrite(w.buf.data(), 1, w.buf.size(), f) == w.buf.size();
+  ok = ok && std::fwrite(&sum, 1, sizeof sum, f) == sizeof sum;
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) err = path + ": write failed";
+  return ok;
+}
+
+bool load_profiles_binary(const std::string& path, std::vector<ProfileHost>& out, std::string& err, bool& io_error) {
+  io_error = false;
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) {
+    io_error = true;
+    err = path + ": " + std::strerror(errno);
+    return false;
+  }
+  std::vector<uint8_t> all;
+  std::vector<uint8_t> chunk(1 << 16);
+  size_t got;
+  while ((got = std::fread(chunk.data(), 1, chunk.size(), f)) > 0) all.insert(all.end(), chunk.data(), chunk.data() + got);
+  const bool rerr = std::ferror(f) != 0;
+  std::fclose(f);
+  if (rerr) {
+    io_error = true;
+    err = path + ": read failed";
+    return false;
+  }
+  if (all.size() < sizeof kBinMagic + 8 + 8 || std::memcmp(all.data(), kBinMagic, sizeof kBinMagic) != 0) {
+    err = path + ": not a profile cache (bad magic)";
+    return false;
+  }
+  const uint8_t* body = all.data() + sizeof kBinMagic;
+  const size_t nbody = all.size() - sizeof kBinMagic - 8;
+  uint64_t sum = 0;
+  std::memcpy(&sum, body + nbody, 8);
+  if (fnv1a(body, nbody) != sum) {
+    err = path + ": checksum mismatch (truncated or corrupt)";
+    return false;
+  }
+  ByteReader r(body, nbody);
+  uint32_t version = 0, count = 0;
+  if (!r.get(version) || version != kBinVersion) {
+    err = path + ": unsupported cache version " + std::to_string(version);
+    return false;
+  }
+  if (!r.get(count)) {
+    err = path + ": truncated header";
+    return false;
+  }
+  out.clear();
+  out.resize(count);
+  for (uint32_t i = 0; i < count; i++) {
+    ProfileHost& h = out[i];
+    uint8_t has_acc = 0, has_desc = 0, flags = 0;
+    bool ok = r.str(h.name) && r.get(has_acc) && r.str(h.acc) && r.get(has_desc) && r.str(h.desc) && r.get(h.m) &&
+              r.get(flags) && r.raw(h.ga, sizeof h.ga) && r.raw(h.tc, sizeof h.tc) && r.raw(h.nc, sizeof h.nc) &&
+              r.raw(h.msv, sizeof h.msv) && r.raw(h.vit, sizeof h.vit) && r.raw(h.fwd, sizeof h.fwd) &&
+              r.get(h.msv_tbm) && r.raw(h.compo, sizeof h.compo);
+    if (ok && (h.m < 1 || h.m > (1 << 20))) ok = false;
+    const size_t w = ok ? (size_t)h.m + 1 : 0;
+    ok = ok && r.floats(h.msc, NSYM * w) && r.floats(h.mo, NSYM * w);
+    for (int q = 0; q < NTR && ok; q++) ok = r.floats(h.t[q], w);
+    for (int q = 0; q < NTR && ok; q++) ok = r.floats(h.p[q], w);
+    if (!ok) {
+      err = path + ": malformed record for profile " + std::to_string(i);
+      out.clear();
+      return false;
+    }
+    h.has_acc = has_acc != 0;
+    h.has_desc = has_desc != 0;
+    h.has_ga = flags & 1;
+    h.has_tc = (flags >> 1) & 1;
+    h.has_nc = (flags >> 2) & 1;
+    h.has_msv = (flags >> 3) & 1;
+    h.has_vit = (flags >> 4) & 1;
+    h.has_fwd = (flags >> 5) & 1;
+  }
+  if (r.left() != 0) {
+    err = path + ": trailing bytes after the last profile";
+    out.clear();
+    return false;
+  }
+  return true;
+}
 
 }  // namespace sx

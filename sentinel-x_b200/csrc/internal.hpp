@@ -57,6 +57,11 @@ bool load_profiles_text(const char* text, size_t len, const std::string& source,
                         std::string& err);
 bool load_profiles_file(const std::string& path, std::vector<ProfileHost>& out, std::string& err, bool& io_error);
 
+// Binary cache of configured profiles (hmmfile.cpp): magic, version, count,
+// the ProfileHost fields of every profile, FNV-1a checksum of the payload.
+bool save_profiles_binary(const std::vector<ProfileHost>& in, const std::string& path, std::string& err);
+bool load_profiles_binary(const std::string& path, std::vector<ProfileHost>& out, std::string& err, bool& io_error);
+
 // Length-dependent special transitions (p7_ReconfigLength; src/hmmer/model.rs:284-312).
 struct SpecialTr {
   float loop, move;    // N/J/C loop and move, log space

@@ -73,6 +73,8 @@ SIGNATURES = {
     "sx_profiles_load_file": (C.c_int, [_P, C.c_char_p, _PP]),
     "sx_profiles_load_text": (C.c_int, [_P, C.c_char_p, C.c_size_t, C.c_char_p, _PP]),
     "sx_profiles_from_arrays": (C.c_int, [_P, C.POINTER(SxProfileArrays), C.c_size_t, _PP]),
+    "sx_profiles_save": (C.c_int, [_P, C.c_char_p]),
+    "sx_profiles_load_binary": (C.c_int, [_P, C.c_char_p, _PP]),
     "sx_profiles_count": (C.c_int32, [_P]),
     "sx_profiles_info": (C.c_int, [_P, C.c_int32, C.POINTER(SxProfileInfo)]),
     "sx_profiles_free": (None, [_P]),
@@ -81,6 +83,8 @@ SIGNATURES = {
     "sx_targets_count": (C.c_int64, [_P]),
     "sx_targets_free": (None, [_P]),
     "sx_search": (C.c_int, [_P, _P, _P, C.POINTER(SxSearchCfg), _PP]),
+    "sx_search_many": (C.c_int, [_P, C.POINTER(C.c_void_p), C.c_size_t, _P, C.POINTER(SxSearchCfg),
+                                 C.POINTER(C.c_void_p)]),
     "sx_hits_count": (C.c_size_t, [_P]),
     "sx_hits_array": (C.POINTER(SxHit), [_P]),
     "sx_hits_domain_count": (C.c_size_t, [_P]),
@@ -181,14 +185,20 @@ class Engine:
         """Raw sx_search -> (hits structured array, domains structured array)."""
         out = C.c_void_p()
         _check(_lib.sx_search(self.h, profiles.h, targets.h, C.byref(cfg), C.byref(out)))
-        try:
-            nh = _lib.sx_hits_count(out)
-            nd = _lib.sx_hits_domain_count(out)
-            hits = [_copy(_lib.sx_hits_array(out)[i]) for i in range(nh)]
-            doms = [_copy(_lib.sx_hits_domains(out)[i]) for i in range(nd)]
-        finally:
-            _lib.sx_hits_free(out)
-        return hits, doms
+        return _take_hits(out)
+
+    def search_many(self, sets, targets, cfg):
+        """sx_search_many: one device search over several profile sets; a list
+        with (hits, domains) per set, as search() would return for each."""
+        n = len(sets)
+        arr = (C.c_void_p * max(n, 1))(*[s.h for s in sets])
+        outs = (C.c_void_p * max(n, 1))()
+        _check(_lib.sx_search_many(self.h, arr, n, targets.h, C.byref(cfg), outs))
+        return [_take_hits(C.c_void_p(outs[i])) for i in range(n)]
+
+    def load_binary(self, path):
+        """Profiles from a cache written by Profiles.save (sx_profiles_load_binary)."""
+        return Profiles(self, binary=path)
 
     def stats(self):
         s = SxSearchStats()
@@ -223,6 +233,17 @@ class Engine:
         return lnz, d_msc, d_isc, d_tr
 
 
+def _take_hits(out):
+    try:
+        nh = _lib.sx_hits_count(out)
+        nd = _lib.sx_hits_domain_count(out)
+        hits = [_copy(_lib.sx_hits_array(out)[i]) for i in range(nh)]
+        doms = [_copy(_lib.sx_hits_domains(out)[i]) for i in range(nd)]
+    finally:
+        _lib.sx_hits_free(out)
+    return hits, doms
+
+
 def _copy(s):
     c = type(s)()
     C.pointer(c)[0] = s
@@ -232,10 +253,12 @@ def _copy(s):
 class Profiles:
     """A configured profile set on the device (sx_profiles)."""
 
-    def __init__(self, engine, text=None, path=None, source="<stream>", arrays=None):
+    def __init__(self, engine, text=None, path=None, source="<stream>", arrays=None, binary=None):
         self.engine = engine
         h = C.c_void_p()
-        if arrays is not None:
+        if binary is not None:
+            _check(_lib.sx_profiles_load_binary(engine.h, os.fsencode(binary), C.byref(h)))
+        elif arrays is not None:
             keep, recs = [], (SxProfileArrays * max(1, len(arrays)))()
             for i, a in enumerate(arrays):
                 m = int(a["m"])
@@ -285,6 +308,10 @@ class Profiles:
 
     def __len__(self):
         return self.n
+
+    def save(self, path):
+        """Write the configured set as a binary cache (sx_profiles_save)."""
+        _check(_lib.sx_profiles_save(self.h, os.fsencode(path)))
 
     def close(self):
         if getattr(self, "h", None):

@@ -211,6 +211,83 @@ def test_profiles_from_arrays_same_as_text(engine):
         engine.load_arrays([bad])
 
 
+def _raw(hits_doms):
+    hits, doms = hits_doms
+    out = []
+    for h in hits:
+        ds = doms[h.domain_offset:h.domain_offset + h.ndomains]
+        out.append((h.profile_index, h.target_index, h.qlen, h.tlen, h.score, h.bias, h.evalue, h.nexpected,
+                    [(d.score, d.bias, d.c_evalue, d.i_evalue, d.hmm_from, d.hmm_to, d.ali_from, d.ali_to,
+                      d.env_from, d.env_to, d.reported) for d in ds]))
+    return out
+
+
+def _same_info(a, b):
+    assert len(a) == len(b)
+    for x, y in zip(a, b):
+        for k in x:
+            if isinstance(x[k], tuple):
+                assert np.array_equal(np.array(x[k]), np.array(y[k]), equal_nan=True), k
+            else:
+                assert x[k] == y[k], k
+
+
+def _digital(engine, w):
+    lens = np.array([len(x) for x in w.targets], np.int64)
+    offs = np.zeros(len(lens), np.int64)
+    offs[1:] = np.cumsum(lens)[:-1]
+    return engine.targets_digital(np.concatenate(w.targets), offs, lens)
+
+
+def test_search_many_equals_separate_searches(engine):
+    """sx_search_many over several profile sets returns, per set, exactly
+    what separate sx_search calls return (how BUSCO/CheckV batch their files)."""
+    from sxhmm import synth
+    w = small_config(1, 0.01)
+    sets = [engine.load_text(synth.profile_text(p)) for p in w.profiles[:5]]
+    sets.append(engine.load_text("".join(synth.profile_text(p) for p in w.profiles[5:9])))
+    ts = _digital(engine, w)
+    for cut in (sxhmm.Cutoff.evalue(10.0, 10.0), sxhmm.Cutoff.gathering()):
+        cfg = sxhmm.SearchConfig(cut).to_c()
+        many = engine.search_many(sets, ts, cfg)
+        assert len(many) == len(sets)
+        for s, got in zip(sets, many):
+            assert _raw(got) == _raw(engine.search(s, ts, cfg))
+        assert sum(len(h) for h, _ in many) > 0
+    tiny = engine.load_text(tiny_text())
+    with pytest.raises(sxhmm.HmmError, match="TC bit thresholds unavailable on model tiny"):
+        engine.search_many([sets[0], tiny], ts, sxhmm.SearchConfig(sxhmm.Cutoff.trusted()).to_c())
+
+
+def test_profile_cache_round_trip(engine, tmp_path):
+    """A set written by sx_profiles_save and read by sx_profiles_load_binary
+    searches exactly like the parsed file; damaged caches are refused."""
+    w = small_config(1, 0.01)
+    text = w.hmm_text()
+    ps = engine.load_text(text)
+    path = tmp_path / "lib.sxp"
+    ps.save(str(path))
+    pb = engine.load_binary(str(path))
+    _same_info(pb.info, ps.info)
+    ts = _digital(engine, w)
+    cfg = sxhmm.SearchConfig().to_c()
+    assert _raw(engine.search(pb, ts, cfg)) == _raw(engine.search(ps, ts, cfg))
+    data = path.read_bytes()
+    bad = bytearray(data)
+    bad[len(bad) // 2] ^= 0x40
+    (tmp_path / "flip.sxp").write_bytes(bytes(bad))
+    with pytest.raises(sxhmm.HmmError, match="checksum mismatch"):
+        engine.load_binary(str(tmp_path / "flip.sxp"))
+    (tmp_path / "cut.sxp").write_bytes(data[: len(data) // 3])
+    with pytest.raises(sxhmm.HmmError, match="checksum mismatch|bad magic"):
+        engine.load_binary(str(tmp_path / "cut.sxp"))
+    (tmp_path / "text.sxp").write_bytes(text.encode()[:4096])
+    with pytest.raises(sxhmm.HmmError, match="bad magic"):
+        engine.load_binary(str(tmp_path / "text.sxp"))
+    with pytest.raises(sxhmm.HmmError):
+        engine.load_binary(str(tmp_path / "missing.sxp"))
+
+
 def test_digital_targets_validated(engine):
     """Digitised targets: a code above 24 ('*') is rejected with its position;
     the same residues as text and as codes give the same scores."""

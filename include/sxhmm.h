@@ -42,6 +42,11 @@ extern "C" {
 
 /* Engine options. */
 #define SX_FLAG_PLAIN 1u /* run the plain one-pair-per-block kernels instead of the batched cascade */
+/* Where the envelope rescoring of domain definition runs (default: chosen per
+ * profile block; the device when the host's share would not hide behind the
+ * device cascade).  Results are identical either way. */
+#define SX_FLAG_ENV_DEVICE 2u /* always on the device */
+#define SX_FLAG_ENV_HOST 4u   /* always on the host */
 
 typedef struct sx_engine sx_engine;
 typedef struct sx_profiles sx_profiles;
@@ -188,9 +193,10 @@ void sx_hits_free(sx_hits* h);
  * leaving each stage, DP cells per stage and milliseconds per stage.
  * stage: 0 MSV, 1 bias, 2 Viterbi, 3 Forward pre-screen (device, CUDA
  * events), 4 Forward/Backward row passes of the final pairs (device + copies),
- * 5 host domain definition (busy time of the host pool, which overlaps the
+ * 5 domain definition (busy time of the host pool, which overlaps the
  * device stages of later profile blocks), 6 whole call (host clock), 7 host
- * time after the last device work (the part of stage 5 not hidden). */
+ * time after the last device work (the part of stage 5 not hidden).
+ * pairs_out[5] counts the envelopes rescored by the device passes. */
 typedef struct {
   int64_t pairs_in[8], pairs_out[8];
   double cells[8];

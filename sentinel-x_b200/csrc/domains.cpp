@@ -428,6 +428,7 @@ class EnvelopeScorer {
         k = pick;
         s1 = pst;
       } else if (s0 == SM) {
+        if (i < 1 || k < 1) break;  // no predecessor left (reachable only when every path is -inf)
         if (!got_last) { got_last = true; cd.i1 = i; cd.k1 = k; }
         got_first = true;
         cd.i0 = i;
@@ -446,6 +447,7 @@ class EnvelopeScorer {
         i -= 1;
         s1 = best == 0 ? SM : best == 1 ? SI : best == 2 ? SD : SB;
       } else if (s0 == SD) {
+        if (k < 1) break;
         const size_t row = (size_t)i * w_;
         float a = kNegInf, b = kNegInf;
         if (k >= 2) {
@@ -455,6 +457,7 @@ class EnvelopeScorer {
         k -= 1;
         s1 = a >= b ? SM : SD;
       } else if (s0 == SI) {
+        if (i < 1 || k < 1) break;
         const size_t prow = (size_t)(i - 1) * w_;
         const float a = dis(pmi[k], om_[prow + k]);
         const float b = dis(pii[k], oi_[prow + k]);
@@ -932,57 +935,17 @@ float backward_score_from_rows(int64_t l, const float* bwd_rows) {
   return backward_log_rows(l, bwd_rows, sp);
 }
 
-bool define_domains(const ProfileHost& p, const uint8_t* dsq, int64_t l, const RawRows& rows, float fwdsc,
-                    const SearchOpts& o, HitOut& out) {
-  if (!std::isfinite(fwdsc)) return false;
-  const SpecialTr xs = special_transitions(l, true);
-  LogRows f, b;
-  double lnscale_f;
-  forward_log_rows(p, l, rows.fwd, f, lnscale_f);
-  const float bcksc = backward_log_rows(l, rows.bwd, b);
-  const float overall = std::isfinite(bcksc) ? bcksc : fwdsc;
-  const float nullsc = null1_score(l);
+namespace {
 
-  // posterior decoding of the special states (p7_GDomainDecoding)
-  std::vector<float> btot((size_t)l + 1, 0.0f), etot((size_t)l + 1, 0.0f), mocc((size_t)l + 1, 0.0f);
-  for (int64_t i = 1; i <= l; i++) {
-    btot[i] = btot[i - 1] + std::exp(f.b[i - 1] + b.b[i - 1] - overall);
-    etot[i] = etot[i - 1] + std::exp(f.e[i] + b.e[i] - overall);
-    const float njc = std::exp(f.n[i - 1] + b.n[i] + xs.loop - overall) +
-                      std::exp(f.j[i - 1] + b.j[i] + xs.loop - overall) +
-                      std::exp(f.c[i - 1] + b.c[i] + xs.loop - overall);
-    mocc[i] = 1.0f - njc;
-  }
-  out.nexpected = btot[l];
+struct Env {
+  DomainOut d;
+  float envsc, domcorr;
+};
 
-  // region identification (p7_domaindef_ByPosteriorHeuristics)
-  EnvelopeScorer es(p, dsq, l, o);
-  std::vector<float> n2sc((size_t)l + 1, 0.0f);
-  struct Env { DomainOut d; float envsc, domcorr; };
-  std::vector<Env> envs;
-  int64_t nregions = 0, start = -1;
-  bool triggered = false;
-  for (int64_t j = 1; j <= l; j++) {
-    if (!triggered) {
-      if (mocc[j] - (btot[j] - btot[j - 1]) < 0.10f || start == -1) start = j;
-      if (mocc[j] >= 0.25f) triggered = true;
-    } else if (mocc[j] - (etot[j] - etot[j - 1]) < 0.10f) {
-      const int64_t ri = std::max<int64_t>(start, 1);
-      nregions++;
-      Env e;
-      if (is_multidomain(btot, etot, ri, j)) {
-        for (auto [ei, ej] : es.trace_ensemble(ri, j, n2sc))
-          if (es.rescore(ei, ej, n2sc, true, e.d, e.envsc, e.domcorr)) envs.push_back(e);
-      } else if (es.rescore(ri, j, n2sc, false, e.d, e.envsc, e.domcorr)) {
-        envs.push_back(e);
-      }
-      start = -1;
-      triggered = false;
-    }
-  }
-  if (nregions == 0 || envs.empty()) return false;
-
-  // sequence and domain scores
+// Sequence and domain scores of a pair from its rescored envelopes
+// (src/hmmer/pipeline.rs:247-293).
+void assemble_hit(const ProfileHost& p, int64_t l, float fwdsc, float nullsc, int64_t nregions,
+                  const std::vector<float>& n2sc, const std::vector<Env>& envs, const SearchOpts& o, HitOut& out) {
   const float omega = std::log(1.0f / 256.0f);
   float seqbias = 0.0f;
   if (o.null2) {
@@ -1026,8 +989,255 @@ bool define_domains(const ProfileHost& p, const uint8_t* dsq, int64_t l, const R
     d.lnp = p.has_fwd ? exp_tail_logsurv((double)d.bits, ftau, flam) : NAN;
     out.domains.push_back(d);
   }
+}
+
+}  // namespace
+
+namespace {
+
+// Posterior decoding of the special states and region identification
+// (p7_GDomainDecoding + p7_domaindef_ByPosteriorHeuristics,
+// src/hmmer/pipeline.rs:187-245): calls on_region(i, j, multidomain) for each
+// region in order.  Returns false when fwdsc is not finite.
+template <typename F>
+bool decode_regions(const ProfileHost& p, int64_t l, const RawRows& rows, float fwdsc, float& nexpected,
+                    F&& on_region) {
+  if (!std::isfinite(fwdsc)) return false;
+  const SpecialTr xs = special_transitions(l, true);
+  LogRows f, b;
+  double lnscale_f;
+  forward_log_rows(p, l, rows.fwd, f, lnscale_f);
+  const float bcksc = backward_log_rows(l, rows.bwd, b);
+  const float overall = std::isfinite(bcksc) ? bcksc : fwdsc;
+  std::vector<float> btot((size_t)l + 1, 0.0f), etot((size_t)l + 1, 0.0f), mocc((size_t)l + 1, 0.0f);
+  for (int64_t i = 1; i <= l; i++) {
+    btot[i] = btot[i - 1] + std::exp(f.b[i - 1] + b.b[i - 1] - overall);
+    etot[i] = etot[i - 1] + std::exp(f.e[i] + b.e[i] - overall);
+    const float njc = std::exp(f.n[i - 1] + b.n[i] + xs.loop - overall) +
+                      std::exp(f.j[i - 1] + b.j[i] + xs.loop - overall) +
+                      std::exp(f.c[i - 1] + b.c[i] + xs.loop - overall);
+    mocc[i] = 1.0f - njc;
+  }
+  nexpected = btot[l];
+  int64_t start = -1;
+  bool triggered = false;
+  for (int64_t j = 1; j <= l; j++) {
+    if (!triggered) {
+      if (mocc[j] - (btot[j] - btot[j - 1]) < 0.10f || start == -1) start = j;
+      if (mocc[j] >= 0.25f) triggered = true;
+    } else if (mocc[j] - (etot[j] - etot[j - 1]) < 0.10f) {
+      const int64_t ri = std::max<int64_t>(start, 1);
+      on_region(ri, j, is_multidomain(btot, etot, ri, j));
+      start = -1;
+      triggered = false;
+    }
+  }
   return true;
 }
+
+}  // namespace
+
+bool define_domains(const ProfileHost& p, const uint8_t* dsq, int64_t l, const RawRows& rows, float fwdsc,
+                    const SearchOpts& o, HitOut& out) {
+  EnvelopeScorer es(p, dsq, l, o);
+  std::vector<float> n2sc((size_t)l + 1, 0.0f);
+  std::vector<Env> envs;
+  int64_t nregions = 0;
+  const bool ok = decode_regions(p, l, rows, fwdsc, out.nexpected, [&](int64_t ri, int64_t j, bool multi) {
+    nregions++;
+    Env e;
+    if (multi) {
+      for (auto [ei, ej] : es.trace_ensemble(ri, j, n2sc))
+        if (es.rescore(ei, ej, n2sc, true, e.d, e.envsc, e.domcorr)) envs.push_back(e);
+    } else if (es.rescore(ri, j, n2sc, false, e.d, e.envsc, e.domcorr)) {
+      envs.push_back(e);
+    }
+  });
+  if (!ok || nregions == 0 || envs.empty()) return false;
+  assemble_hit(p, l, fwdsc, null1_score(l), nregions, n2sc, envs, o, out);
+  return true;
+}
+
+// ---- batched domain definition (device envelope passes) ----------------------
+struct DomainBatch::Impl {
+  struct Pending {
+    int64_t i, j;
+    bool null2_done;
+    bool pass;         // false: rescore rejects the envelope before any pass
+    int64_t req = -1;  // index into reqs
+  };
+  struct PairState {
+    bool begun = false;
+    const ProfileHost* p = nullptr;
+    const uint8_t* dsq = nullptr;
+    int64_t l = 0;
+    int32_t pi = 0, ti = 0;
+    float fwdsc = 0, nexpected = 0;
+    int64_t nregions = 0;
+    std::vector<float> n2sc;
+    std::vector<Pending> pend;
+  };
+  SearchOpts o;
+  std::vector<PairState> pairs;
+  std::vector<EnvRequest> reqs;
+};
+
+DomainBatch::DomainBatch(const SearchOpts& o, size_t npairs) : impl_(new Impl) {
+  impl_->o = o;
+  impl_->pairs.resize(npairs);
+}
+DomainBatch::~DomainBatch() = default;
+
+void DomainBatch::begin(size_t q, const ProfileHost& p, int32_t pi, const uint8_t* dsq, int64_t l, int32_t ti,
+                        const RawRows& rows, float fwdsc) {
+  Impl::PairState& st = impl_->pairs[q];
+  st.p = &p;
+  st.dsq = dsq;
+  st.l = l;
+  st.pi = pi;
+  st.ti = ti;
+  st.fwdsc = fwdsc;
+  st.n2sc.assign((size_t)l + 1, 0.0f);
+  EnvelopeScorer es(p, dsq, l, impl_->o);
+  auto add = [&](int64_t i, int64_t j, bool null2_done) {
+    st.pend.push_back({i, j, null2_done, !(i == 0 || j < i || j > l), -1});
+  };
+  st.begun = decode_regions(p, l, rows, fwdsc, st.nexpected, [&](int64_t ri, int64_t j, bool multi) {
+    st.nregions++;
+    if (multi) {  // stochastic traces and clustering stay on the host; their envelopes are batched
+      for (auto [ei, ej] : es.trace_ensemble(ri, j, st.n2sc)) add(ei, ej, true);
+    } else {
+      add(ri, j, false);
+    }
+  });
+}
+
+const std::vector<EnvRequest>& DomainBatch::requests() {
+  Impl& I = *impl_;
+  I.reqs.clear();
+  for (size_t q = 0; q < I.pairs.size(); q++) {
+    Impl::PairState& st = I.pairs[q];
+    if (!st.begun) continue;
+    const SpecialTr uni = special_transitions(st.l, false);
+    for (Impl::Pending& e : st.pend) {
+      if (!e.pass) continue;
+      e.req = (int64_t)I.reqs.size();
+      I.reqs.push_back({(int32_t)q, st.pi, st.ti, e.i, e.j, e.null2_done, uni});
+    }
+  }
+  return I.reqs;
+}
+
+// forward_matrix's score and backward_matrix's row 0 from the raw rows, then
+// decode's per-row factor and N/J/C posteriors (src/hmmer/dp.rs:442-601,
+// 1278-1306), with the libm the reference uses.
+void DomainBatch::factors(size_t r, const float* fr, const float* br, EnvFactors& f) const {
+  const EnvRequest& q = impl_->reqs[r];
+  const SpecialTr& st = q.st;
+  const int64_t lr = q.j - q.i + 1;
+  const size_t n = (size_t)lr + 1;
+  f.ok = false;
+  std::vector<double> lnf(n, 0.0), lnb(n, 0.0);
+  std::vector<float> fn(n, kNegInf), fj(n, kNegInf), fc(n, kNegInf), bn(n, kNegInf), bj(n, kNegInf),
+      bc(n, kNegInf);
+  fn[0] = 0.0f;
+  double lnscale = 0.0;
+  for (int64_t i = 1; i <= lr; i++) {
+    const float* x = fr + 6 * i;
+    if (x[5] > 0.0f) lnscale += std::log((double)x[5]);
+    lnf[i] = lnscale;
+    const float ls = (float)lnscale;
+    fn[i] = lnpos(x[0]) + ls;
+    fj[i] = lnpos(x[3]) + ls;
+    fc[i] = lnpos(x[4]) + ls;
+  }
+  f.envsc = (float)((double)lnpos(fr[6 * lr + 4] * st.pmove) + lnscale);
+  if (!std::isfinite(f.envsc)) return;
+  bc[lr] = lnpos(br[6 * lr + 4]);
+  lnscale = 0.0;
+  for (int64_t i = lr - 1; i >= 1; i--) {
+    const float* x = br + 6 * i;
+    if (x[5] > 0.0f) lnscale += std::log((double)x[5]);
+    lnb[i] = lnscale;
+    const float ls = (float)lnscale;
+    bn[i] = lnpos(x[0]) + ls;
+    bj[i] = lnpos(x[3]) + ls;
+    bc[i] = lnpos(x[4]) + ls;
+  }
+  const float b0 = lnpos(br[1]) + (float)lnscale;
+  const float bsc = logsum2(bn[1] + st.loop, b0 + st.move);
+  if (!std::isfinite(bsc)) return;
+  const double overall = (double)bsc;
+  f.fac.assign(n, 0.0);
+  f.pn.assign(n, 0.0f);
+  f.pj.assign(n, 0.0f);
+  f.pc.assign(n, 0.0f);
+  f.sn = f.sj = f.sc = 0.0f;
+  for (int64_t i = 1; i <= lr; i++) {
+    f.fac[i] = std::exp(lnf[i] + lnb[i] - overall);
+    f.pn[i] = (float)std::exp((double)(fn[i - 1] + bn[i] + st.loop) - overall);
+    f.pj[i] = (float)std::exp((double)(fj[i - 1] + bj[i] + st.loop) - overall);
+    f.pc[i] = (float)std::exp((double)(fc[i - 1] + bc[i] + st.loop) - overall);
+    f.sn += f.pn[i];
+    f.sj += f.pj[i];
+    f.sc += f.pc[i];
+  }
+  f.ok = true;
+}
+
+// The rest of rescore_isolated_domain (src/hmmer/pipeline.rs:545-591) for every
+// envelope of pair q, then the pair's scores.
+bool DomainBatch::finish(size_t q, const std::vector<EnvFactors>& F, const std::vector<EnvDeviceOut>& D,
+                         HitOut& out) {
+  Impl::PairState& st = impl_->pairs[q];
+  const SearchOpts& o = impl_->o;
+  if (!st.begun) return false;
+  out.nexpected = st.nexpected;
+  EnvelopeScorer es(*st.p, st.dsq, st.l, o);
+  const SpecialTr uni = special_transitions(st.l, false);
+  std::vector<Env> envs;
+  for (const Impl::Pending& e : st.pend) {
+    if (e.req < 0) continue;
+    const EnvFactors& f = F[(size_t)e.req];
+    if (!f.ok) continue;
+    const EnvDeviceOut& d = D[(size_t)e.req];
+    const int64_t lr = e.j - e.i + 1;
+    Env v;
+    v.envsc = f.envsc;
+    v.domcorr = 0.0f;
+    if (o.null2) {
+      if (!e.null2_done) {  // null2 by posterior expectation (dp.rs:1310-1350)
+        const float norm = 1.0f / (float)std::max<int64_t>(lr, 1);
+        const float xfactor = f.sn * norm + f.sc * norm + f.sj * norm;
+        const float isum = d.si * norm;
+        float n2[NSYM];
+        for (int x = 0; x < NRES; x++) n2[x] = d.v[x] + isum + xfactor;
+        EnvelopeScorer::average_degenerate(n2);
+        float lg[NSYM];
+        for (int x = 0; x < NSYM; x++) lg[x] = n2[x] > 0.0f ? std::log(n2[x]) : kNegInf;
+        for (int64_t pos = e.i; pos <= e.j; pos++) {
+          const float w = lg[st.dsq[pos - 1]];
+          st.n2sc[pos] = std::isfinite(w) ? w : 0.0f;
+        }
+      }
+      for (int64_t pos = e.i; pos <= e.j; pos++) v.domcorr += st.n2sc[pos];
+    }
+    v.d.ienv = e.i;
+    v.d.jenv = e.j;
+    if (d.found) {
+      v.d.iali = e.i - 1 + d.i0; v.d.jali = e.i - 1 + d.i1; v.d.kali = d.k0; v.d.mali = d.k1;
+    } else if (auto vt = es.viterbi_first(st.dsq + (e.i - 1), lr, uni)) {
+      v.d.iali = e.i - 1 + vt->i0; v.d.jali = e.i - 1 + vt->i1; v.d.kali = vt->k0; v.d.mali = vt->k1;
+    } else {
+      v.d.iali = e.i; v.d.jali = e.j; v.d.kali = 1; v.d.mali = st.p->m;
+    }
+    envs.push_back(v);
+  }
+  if (st.nregions == 0 || envs.empty()) return false;
+  assemble_hit(*st.p, st.l, st.fwdsc, null1_score(st.l), st.nregions, st.n2sc, envs, o, out);
+  return true;
+}
+
 
 float composition_bias_score(const ProfileHost& p, const uint8_t* dsq, int64_t l) {
   const double l0 = 400.0, l1 = (double)p.m / 8.0;

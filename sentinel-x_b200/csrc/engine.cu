@@ -41,6 +41,7 @@
 #include "kernels.cuh"
 #include "adjoint.cuh"
 #include "plain.cuh"
+#include "envelope.cuh"
 
 using namespace sx;
 using sxk::BinRegion;
@@ -206,8 +207,28 @@ struct VbinTable<kNumVbins> {
   static void fill(VitFn*, FwdFn*, BwdFn*, AdjFFn*, AdjBFn*) {}
 };
 
+typedef void (*EnvPassFn)(const sxk::EnvRec*, int, const DevProfile*, const float*, const uint8_t*, const int64_t*,
+                          float*, float*);
+typedef void (*EnvPostFn)(const sxk::EnvRec*, int, const DevProfile*, const float*, float*, float*, const double*,
+                          float*);
+template <int I>
+struct EnvTable {
+  static void fill(EnvPassFn* f, EnvPassFn* b, EnvPostFn* p) {
+    f[I] = sxk::env_forward_kernel<kVcBins[I]>;
+    b[I] = sxk::env_backward_kernel<kVcBins[I]>;
+    p[I] = sxk::env_post_kernel<kVcBins[I]>;
+    EnvTable<I + 1>::fill(f, b, p);
+  }
+};
+template <>
+struct EnvTable<kNumVbins> {
+  static void fill(EnvPassFn*, EnvPassFn*, EnvPostFn*) {}
+};
+
 struct KernelTables {
   MsvFn msv[kNumMsvShapes];
+  EnvPassFn envf[kNumVbins], envb[kNumVbins];
+  EnvPostFn envp[kNumVbins];
   VitFn vit[kNumVbins];
   FwdFn fwd[kNumVbins];
   BwdFn bwd[kNumVbins];
@@ -218,6 +239,7 @@ struct KernelTables {
     MsvTable<0>::fill(msv);
     VitGTable<0>::fill(vitg);
     VbinTable<0>::fill(vit, fwd, bwd, adjf, adjb);
+    EnvTable<0>::fill(envf, envb, envp);
   }
 };
 const KernelTables& kernels() {
@@ -435,11 +457,12 @@ struct Slot {
   void create() {
     int least = 0, greatest = 0;
     CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    // 2 slots x (9 + 7) streams = 32, the most hardware work queues a process
-    // can have (CUDA_DEVICE_MAX_CONNECTIONS=32): with fewer queues, streams
-    // share them and a high-priority launch can wait behind queued MSV work
+    // 2 slots x (9 + 6) streams + 2 envelope streams = 32, the
+    // most hardware work queues a process can have (CUDA_DEVICE_MAX_CONNECTIONS=32):
+    // with fewer queues, streams share them and a high-priority launch can
+    // wait behind queued MSV work
     hi.create(greatest, 8);
-    lo.create(least, 6);
+    lo.create(least, 5);
     for (auto& e : ev) CK(cudaEventCreate(&e));
     CK(cudaEventCreateWithFlags(&msv_done, cudaEventDisableTiming));
   }
@@ -478,6 +501,13 @@ struct sx_engine {
   sx_search_stats stats{};
   int pipeline_blocks = 0;  // profile blocks per search; 0 = by workload size
   BlockPool target_blocks;  // device memory of freed target sets
+  // envelope passes of the host domain definition (used by the host pool's
+  // driver thread, one batch at a time)
+  cudaStream_t env_stream = nullptr, env_stream2 = nullptr;  // Backward runs beside Forward
+  cudaEvent_t env_ev = nullptr;
+  DevBuf<sxk::EnvRec> env_recs;
+  DevBuf<float> env_planes, env_rows, env_aux, env_out;
+  DevBuf<double> env_fac;
   DevBuf<Thresholds> thr;
   DevBuf<float> rows_f, rows_b;
   DevBuf<int64_t> row_off;
@@ -1193,6 +1223,154 @@ double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
+// The device passes of a DomainBatch: for every envelope request the
+// full-matrix Forward and Backward (their raw special rows come back to the
+// host), the host's posterior factors, then the posterior / null2 /
+// optimal-accuracy pass.  One warp per envelope; batches bounded by the
+// memory of their matrix planes.  Runs on the host pool's driver thread.
+// One batch's requests and the places for their results.
+struct EnvSource {
+  const DomainBatch* db;
+  const std::vector<EnvRequest>* reqs;
+  std::vector<EnvFactors>* F;
+  std::vector<EnvDeviceOut>* D;
+};
+
+int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T, std::vector<EnvSource>& srcs,
+                        int nthr) {
+  // every request of every batch, as (batch, request)
+  std::vector<std::pair<uint32_t, uint32_t>> items;
+  for (size_t b = 0; b < srcs.size(); b++) {
+    const size_t nr = srcs[b].reqs->size();
+    srcs[b].F->assign(nr, EnvFactors{});
+    srcs[b].D->assign(nr, EnvDeviceOut{});
+    for (size_t r = 0; r < nr; r++) items.emplace_back((uint32_t)b, (uint32_t)r);
+  }
+  const size_t nr = items.size();
+  int64_t launches = 0;
+  if (!nr) return 0;
+  auto req = [&](size_t x) -> const EnvRequest& { return (*srcs[items[x].first].reqs)[items[x].second]; };
+  auto fac_of = [&](size_t x) -> EnvFactors& { return (*srcs[items[x].first].F)[items[x].second]; };
+  auto out_of = [&](size_t x) -> EnvDeviceOut& { return (*srcs[items[x].first].D)[items[x].second]; };
+  const auto& K = kernels();
+  cudaStream_t s = E->env_stream;
+  const int64_t budget = std::max<int64_t>(E->batch_bytes / 2, 256LL << 20);
+  std::vector<size_t> order(nr);
+  std::iota(order.begin(), order.end(), (size_t)0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](size_t x, size_t y) { return P->dp[req(x).p].vbin < P->dp[req(y).p].vbin; });
+  size_t a = 0;
+  while (a < nr) {
+    size_t b = a;
+    int64_t planes = 0, rowsz = 0, aux = 0, fac = 0;
+    std::vector<sxk::EnvRec> recs;
+    while (b < nr) {
+      const EnvRequest& q = req(order[b]);
+      const int vc = kVcBins[P->dp[q.p].vbin];
+      const int64_t lr = q.j - q.i + 1;
+      const int64_t need = 5 * (lr + 1) * 32 * vc;
+      if (b > a && (planes + need) * (int64_t)sizeof(float) > budget) break;
+      sxk::EnvRec r{};
+      r.p = q.p;
+      r.t = q.t;
+      r.i0 = (int32_t)(q.i - 1);
+      r.lr = (int32_t)lr;
+      r.ploop = q.st.ploop;
+      r.pmove = q.st.pmove;
+      r.pe_loop = q.st.pe_loop;
+      r.pe_move = q.st.pe_move;
+      r.plane_off = planes;
+      r.row_off = rowsz;
+      r.aux_off = aux;
+      r.fac_off = fac;
+      r.out_off = (int64_t)(b - a) * sxk::kEnvOut;
+      planes += need;
+      rowsz += 12 * (lr + 1);
+      aux += 8 * (lr + 1);
+      fac += lr + 1;
+      recs.push_back(r);
+      b++;
+    }
+    const size_t n = b - a;
+    E->env_recs.upload(recs.data(), n, s);
+    E->env_planes.alloc((size_t)planes);
+    E->env_rows.alloc((size_t)rowsz);
+    E->env_aux.alloc((size_t)aux);
+    E->env_fac.alloc((size_t)fac);
+    E->env_out.alloc(n * sxk::kEnvOut);
+    // one launch per vbin: requests are sorted by vbin
+    auto each_bin = [&](auto&& launch) {
+      size_t x = 0;
+      while (x < n) {
+        const int vb = P->dp[req(order[a + x]).p].vbin;
+        size_t y = x;
+        while (y < n && P->dp[req(order[a + y]).p].vbin == vb) y++;
+        const int cnt = (int)(y - x);
+        launch(vb, (int)x, cnt, (int)std::min<int64_t>(cnt, (int64_t)E->num_sms * 32));
+        x = y;
+      }
+    };
+    // Forward on the envelope stream, Backward beside it on the second one
+    CK(cudaEventRecord(E->env_ev, s));
+    CK(cudaStreamWaitEvent(E->env_stream2, E->env_ev, 0));
+    each_bin([&](int vb, int x0, int cnt, int blocks) {
+      K.envf[vb]<<<blocks, 32, 0, s>>>(E->env_recs.p + x0, cnt, P->d_prof.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
+                                       E->env_planes.p, E->env_rows.p);
+      K.envb[vb]<<<blocks, 32, 0, E->env_stream2>>>(E->env_recs.p + x0, cnt, P->d_prof.p, P->d_vfb.p, T->d_res.p,
+                                                    T->d_off.p, E->env_planes.p, E->env_rows.p);
+      launches += 2;
+    });
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(E->env_ev, E->env_stream2));
+    CK(cudaStreamWaitEvent(s, E->env_ev, 0));
+    std::vector<float> hrows((size_t)rowsz);
+    CK(cudaMemcpyAsync(hrows.data(), E->env_rows.p, sizeof(float) * (size_t)rowsz, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    parallel_for(n, nthr, [&](size_t x) {
+      const sxk::EnvRec& r = recs[x];
+      const auto& it = items[order[a + x]];
+      srcs[it.first].db->factors(it.second, hrows.data() + r.row_off,
+                                 hrows.data() + r.row_off + 6 * ((int64_t)r.lr + 1), fac_of(order[a + x]));
+    });
+    std::vector<float> haux((size_t)aux, 0.0f);
+    std::vector<double> hfac((size_t)fac, 0.0);
+    for (size_t x = 0; x < n; x++) {
+      const EnvFactors& f = fac_of(order[a + x]);
+      if (!f.ok) continue;
+      const sxk::EnvRec& r = recs[x];
+      const size_t w = (size_t)r.lr + 1;
+      std::copy(f.pn.begin(), f.pn.end(), haux.begin() + r.aux_off);
+      std::copy(f.pj.begin(), f.pj.end(), haux.begin() + r.aux_off + w);
+      std::copy(f.pc.begin(), f.pc.end(), haux.begin() + r.aux_off + 2 * w);
+      std::copy(f.fac.begin(), f.fac.end(), hfac.begin() + r.fac_off);
+    }
+    CK(cudaMemcpyAsync(E->env_aux.p, haux.data(), sizeof(float) * (size_t)aux, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(E->env_fac.p, hfac.data(), sizeof(double) * (size_t)fac, cudaMemcpyHostToDevice, s));
+    each_bin([&](int vb, int x0, int cnt, int blocks) {
+      K.envp[vb]<<<blocks, 32, 0, s>>>(E->env_recs.p + x0, cnt, P->d_prof.p, P->d_vfb.p, E->env_planes.p,
+                                       E->env_aux.p, E->env_fac.p, E->env_out.p);
+      launches += 1;
+    });
+    CK(cudaGetLastError());
+    std::vector<float> hout(n * sxk::kEnvOut);
+    CK(cudaMemcpyAsync(hout.data(), E->env_out.p, sizeof(float) * hout.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (size_t x = 0; x < n; x++) {
+      const float* o = hout.data() + x * sxk::kEnvOut;
+      EnvDeviceOut& d = out_of(order[a + x]);
+      for (int k = 0; k < NRES; k++) d.v[k] = o[k];
+      d.si = o[20];
+      d.found = o[21] != 0.0f;
+      d.i0 = (int32_t)o[22];
+      d.i1 = (int32_t)o[23];
+      d.k0 = (int32_t)o[24];
+      d.k1 = (int32_t)o[25];
+    }
+    a = b;
+  }
+  return launches;
+}
+
 // Contiguous ranges of profile indices with about equal filtered DP cells.
 // Each range runs through the device cascade as one block; the host domain
 // definition of a block overlaps the device work of the blocks after it.
@@ -1418,40 +1596,114 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
   std::vector<std::unique_ptr<BlockOut>> outs;
   std::atomic<int64_t> n_domain{0};
   double rows_ms = 0;
-  // F3 and domain definition of one final pair (pipeline.rs:179-293)
-  auto define_pair = [&](BlockOut* B, size_t i, const float* fr, const float* br) {
-    const FinalPair& f = B->finals[i];
-    const ProfileHost& h = P->h[f.p];
-    const int64_t l = T->len[f.t];
-    const float fwdsc = forward_score_from_rows(h, l, fr);
-    if (th[f.p].exact) {  // F3 (pipeline.rs:179-183)
-      if (std::exp(exp_tail_logsurv((double)((fwdsc - f.filtersc) / kLn2f), h.fwd[0], h.fwd[1])) > o.f3) return;
-    }
-    n_domain++;
-    RawRows rr{fr, br};
-    B->res[i].hit = define_domains(h, T->dsq.data() + T->off[f.t], l, rr, fwdsc, o, B->res[i].h);
+  // errors raised on the host pool's thread, reported after it is joined
+  std::mutex host_err_mu;
+  int host_err_code = 0;
+  std::string host_err_msg;
+  std::atomic<int64_t> n_env{0}, env_launches{0};
+  // batches whose host phase is done; their envelope passes run after the cascade
+  struct PendingBatch {
+    BlockOut* B;
+    std::vector<size_t> which;
+    std::vector<char> begun;
+    std::unique_ptr<DomainBatch> db;
+    std::vector<EnvRequest> reqs;
+    std::vector<EnvFactors> F;
+    std::vector<EnvDeviceOut> D;
   };
+  std::vector<std::unique_ptr<PendingBatch>> pending;  // appended by the pool's driver thread only
   HostQueue hq(E->host_threads);  // declared after what its jobs use, so it is joined first
   // device rows of a block's final pairs; their domain definition is queued
   // and runs while the engine thread moves on to the next block
-  auto rows_and_queue = [&](Slot& S, BlockOut* B) {
+  // Domain definition of a block runs on the host pool, hidden behind the
+  // device work of later blocks, while that host work stays well below the
+  // block's device time; past that (hit-heavy blocks) the envelopes' full-
+  // matrix passes go to the device.  Host: ~44 ns per DP cell of the final
+  // pairs per thread; device cascade ~4.4e12 cells/s (B200, Pfam-scale).
+  auto device_envelopes = [&](const BlockOut* B, double block_cells) {
+    if (E->flags & SX_FLAG_ENV_DEVICE) return true;
+    if (E->flags & SX_FLAG_ENV_HOST) return false;
+    double fin = 0;
+    for (const auto& f : B->finals) fin += (double)P->h[f.p].m * (double)T->len[f.t];
+    const double host_ms = fin * 44e-9 * 1e3 / std::max(1, E->host_threads);
+    const double dev_ms = block_cells / 4.4e12 * 1e3;
+    return host_ms > 0.5 * dev_ms + 5.0;
+  };
+  auto rows_and_queue = [&](Slot& S, BlockOut* B, bool dev_env) {
     B->res.resize(B->finals.size());
     const auto t0 = std::chrono::steady_clock::now();
-    rows_pass(E, S, P, T, B->finals, [&, B](RowsChunk&& c) {
+    rows_pass(E, S, P, T, B->finals, [&, B, dev_env](RowsChunk&& c) {
       auto ch = std::make_shared<RowsChunk>(std::move(c));
-      hq.push([&, B, ch](int nthr) {
-        // largest pairs first, for an even finish across the workers
-        std::vector<size_t> ord(ch->which.size());
-        std::iota(ord.begin(), ord.end(), (size_t)0);
-        auto cost = [&](size_t q) {
-          const FinalPair& f = B->finals[ch->which[q]];
-          return (double)P->h[f.p].m * (double)T->len[f.t];
-        };
-        std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return cost(a) > cost(b); });
-        parallel_for(ord.size(), nthr, [&](size_t r) {
-          const size_t q = ord[r];
-          define_pair(B, ch->which[q], ch->f.data() + ch->off[q], ch->b.data() + ch->off[q]);
-        });
+      hq.push([&, B, ch, dev_env](int nthr) {
+        try {
+          const size_t nq = ch->which.size();
+          // largest pairs first, for an even finish across the workers
+          std::vector<size_t> ord(nq);
+          std::iota(ord.begin(), ord.end(), (size_t)0);
+          auto cost = [&](size_t q) {
+            const FinalPair& f = B->finals[ch->which[q]];
+            return (double)P->h[f.p].m * (double)T->len[f.t];
+          };
+          std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return cost(a) > cost(b); });
+          if (!dev_env) {  // F3 and the whole domain definition on the host (pipeline.rs:179-293)
+            parallel_for(ord.size(), nthr, [&](size_t rr) {
+              const size_t q = ord[rr];
+              const size_t i = ch->which[q];
+              const FinalPair& f = B->finals[i];
+              const ProfileHost& h = P->h[f.p];
+              const int64_t l = T->len[f.t];
+              const float* fr = ch->f.data() + ch->off[q];
+              const float* br = ch->b.data() + ch->off[q];
+              const float fwdsc = forward_score_from_rows(h, l, fr);
+              if (th[f.p].exact &&
+                  std::exp(exp_tail_logsurv((double)((fwdsc - f.filtersc) / kLn2f), h.fwd[0], h.fwd[1])) > o.f3)
+                return;
+              n_domain++;
+              B->res[i].hit = define_domains(h, T->dsq.data() + T->off[f.t], l, RawRows{fr, br}, fwdsc, o, B->res[i].h);
+            });
+            return;
+          }
+          // F3 (pipeline.rs:179-183), posterior decoding, regions and the
+          // stochastic traces of multi-domain regions on the host; the
+          // envelopes' full-matrix passes wait until the cascade is done
+          auto pb = std::make_unique<PendingBatch>();
+          pb->B = B;
+          pb->which = ch->which;
+          pb->begun.assign(nq, 0);
+          pb->db = std::make_unique<DomainBatch>(o, nq);
+          DomainBatch& db = *pb->db;
+          std::vector<char>& begun = pb->begun;
+          parallel_for(ord.size(), nthr, [&](size_t rr) {
+            const size_t q = ord[rr];
+            const FinalPair& f = B->finals[ch->which[q]];
+            const ProfileHost& h = P->h[f.p];
+            const int64_t l = T->len[f.t];
+            const float* fr = ch->f.data() + ch->off[q];
+            const float* br = ch->b.data() + ch->off[q];
+            const float fwdsc = forward_score_from_rows(h, l, fr);
+            if (th[f.p].exact &&
+                std::exp(exp_tail_logsurv((double)((fwdsc - f.filtersc) / kLn2f), h.fwd[0], h.fwd[1])) > o.f3)
+              return;
+            n_domain++;
+            db.begin(q, h, f.p, T->dsq.data() + T->off[f.t], l, f.t, RawRows{fr, br}, fwdsc);
+            begun[q] = 1;
+          });
+          pb->reqs = db.requests();
+          n_env += (int64_t)pb->reqs.size();
+          pending.push_back(std::move(pb));
+        } catch (const CudaError& ce) {
+          std::lock_guard<std::mutex> g(host_err_mu);
+          if (!host_err_code) {
+            host_err_code = ce.code;
+            host_err_msg = ce.msg;
+          }
+        } catch (const std::bad_alloc&) {
+          std::lock_guard<std::mutex> g(host_err_mu);
+          if (!host_err_code) {
+            host_err_code = SX_ENOMEM;
+            host_err_msg = "sx_search: host allocation failed during domain definition";
+          }
+        }
       });
     });
     rows_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1482,7 +1734,7 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     BlockOut* B = outs.back().get();
     while (!cascade_finish(E, S, P, T, th, o, runs[b], B->finals)) cascade_launch(E, S, P, T, th, runs[b]);
     nfinal += (int64_t)B->finals.size();
-    rows_and_queue(S, B);
+    rows_and_queue(S, B, device_envelopes(B, runs[b].cells_total));
   }
   if (!unfiltered.empty() && nt > 0) {
     outs.push_back(std::make_unique<BlockOut>());
@@ -1490,10 +1742,32 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     for (int pi : unfiltered)
       for (size_t t = 0; t < nt; t++) B->finals.push_back({pi, (int32_t)t, 0.f, 0.f, 0.f, -1});
     nfinal += (int64_t)B->finals.size();
-    rows_and_queue(E->sl[0], B);
+    rows_and_queue(E->sl[0], B, !(E->flags & SX_FLAG_ENV_HOST));  // every pair reaches domain definition
   }
   const auto t_dev = std::chrono::steady_clock::now();
   E->stats.ms[5] = hq.finish();
+  if (host_err_code) return fail(host_err_code, host_err_msg);
+  // every envelope of the search through the device passes at once, on an
+  // idle GPU, then each pair's scores
+  {
+    const auto t_env = std::chrono::steady_clock::now();
+    std::vector<EnvSource> srcs;
+    for (auto& pb : pending) srcs.push_back({pb->db.get(), &pb->reqs, &pb->F, &pb->D});
+    env_launches += envelope_passes(E, P, T, srcs, E->host_threads);
+    std::vector<std::pair<PendingBatch*, size_t>> todo;
+    for (auto& pb : pending)
+      for (size_t q = 0; q < pb->which.size(); q++)
+        if (pb->begun[q]) todo.emplace_back(pb.get(), q);
+    parallel_for(todo.size(), E->host_threads, [&](size_t x) {
+      PendingBatch& pb = *todo[x].first;
+      const size_t q = todo[x].second;
+      const size_t i = pb.which[q];
+      pb.B->res[i].hit = pb.db->finish(q, pb.F, pb.D, pb.B->res[i].h);
+    });
+    E->stats.ms[5] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_env).count();
+  }
+  E->stats.kernel_launches += env_launches.load();
+  E->stats.pairs_out[5] = n_env.load();
   const auto t_end = std::chrono::steady_clock::now();
   E->stats.pairs_in[4] = nfinal;
   E->stats.pairs_out[4] = n_domain.load();
@@ -1541,6 +1815,13 @@ int sx_create(const sx_opts* opts, sx_engine** out) {
                                  std::to_string(prop.minor) + "); this library is built for sm_100a");
     e->num_sms = prop.multiProcessorCount;
     for (Slot& S : e->sl) S.create();
+    {
+      int least = 0, greatest = 0;
+      CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+      CK(cudaStreamCreateWithPriority(&e->env_stream, cudaStreamNonBlocking, greatest));
+      CK(cudaStreamCreateWithPriority(&e->env_stream2, cudaStreamNonBlocking, greatest));
+      CK(cudaEventCreateWithFlags(&e->env_ev, cudaEventDisableTiming));
+    }
     (void)kernels();
   } catch (const CudaError& ce) {
     return fail(ce.code, ce.msg);
@@ -1553,6 +1834,12 @@ void sx_destroy(sx_engine* e) {
   if (!e) return;
   cudaSetDevice(e->device);
   for (Slot& S : e->sl) S.destroy();
+  for (cudaStream_t st : {e->env_stream, e->env_stream2})
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+  if (e->env_ev) cudaEventDestroy(e->env_ev);
   delete e;
 }
 

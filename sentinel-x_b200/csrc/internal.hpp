@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdint>
 #include <limits>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -106,6 +107,47 @@ struct RawRows {
 // `fwdsc_out` receives the Forward score (for the F3 decision by the caller).
 float forward_score_from_rows(const ProfileHost& p, int64_t l, const float* fwd_rows);
 float backward_score_from_rows(int64_t l, const float* bwd_rows);
+// Batched domain definition: the same results as define_domains, with the
+// full-matrix envelope passes of every pair of a batch done elsewhere (on
+// the device).  Phases: begin() per pair (decoding, regions, stochastic-trace
+// clustering on the host) -> requests() -> the caller runs the Forward and
+// Backward envelope passes -> factors() per request -> the caller runs the
+// posterior / null2 / optimal-accuracy pass -> finish() per pair.
+struct EnvRequest {
+  int32_t pair;     // index of the pair in the batch
+  int32_t p, t;     // profile and target indices
+  int64_t i, j;     // envelope, 1-based residues of the target
+  bool null2_done;  // null2 already set by the region's stochastic traces
+  SpecialTr st;     // unihit special transitions of the target's length
+};
+struct EnvFactors {
+  bool ok = false;  // Forward and Backward envelope scores finite
+  float envsc = 0;
+  std::vector<double> fac;        // exp(lnF[i] + lnB[i] - lnZ), rows 0..lr
+  std::vector<float> pn, pj, pc;  // N/J/C posteriors, rows 0..lr
+  float sn = 0, sj = 0, sc = 0;   // their sums over rows 1..lr, in order
+};
+struct EnvDeviceOut {
+  float v[NRES];  // sum_k (sm[k] * norm) * mo[x][k]
+  float si;       // sum of insert posteriors, row-major
+  bool found;     // optimal-accuracy traceback found a domain
+  int32_t i0, i1, k0, k1;
+};
+class DomainBatch {
+ public:
+  DomainBatch(const SearchOpts& o, size_t npairs);
+  ~DomainBatch();
+  void begin(size_t q, const ProfileHost& p, int32_t pi, const uint8_t* dsq, int64_t l, int32_t ti,
+             const RawRows& rows, float fwdsc);
+  const std::vector<EnvRequest>& requests();
+  void factors(size_t r, const float* fwd_rows, const float* bwd_rows, EnvFactors& f) const;
+  bool finish(size_t q, const std::vector<EnvFactors>& f, const std::vector<EnvDeviceOut>& d, HitOut& out);
+
+ private:
+  struct Impl;
+  std::unique_ptr<Impl> impl_;
+};
+
 bool define_domains(const ProfileHost& p, const uint8_t* dsq, int64_t l, const RawRows& rows, float fwdsc,
                     const SearchOpts& o, HitOut& out);
 

@@ -10,6 +10,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SX_OK, SX_EINVAL, SX_ECUTOFF, SX_ENOMEM, SX_ECUDA, SX_ETIMEOUT, SX_EIO = range(7)
 SX_CUT_EVALUE, SX_CUT_BITS, SX_CUT_GA, SX_CUT_NC, SX_CUT_TC = range(5)
 SX_FLAG_PLAIN = 1
+SX_FLAG_ENV_DEVICE = 2
+SX_FLAG_ENV_HOST = 4
 
 # Every entry point declared in include/sxhmm.h, name -> (restype, argtypes).
 _P = C.c_void_p
@@ -145,9 +147,11 @@ def _ptr(a, t):
 class Engine:
     """One engine per device (sx_create)."""
 
-    def __init__(self, device=0, host_threads=0, plain=False, batch_bytes=0, pipeline_blocks=0):
+    def __init__(self, device=0, host_threads=0, plain=False, batch_bytes=0, pipeline_blocks=0, envelopes="auto"):
         lib = load_library()
-        o = SxOpts(device, host_threads, SX_FLAG_PLAIN if plain else 0, pipeline_blocks, batch_bytes)
+        flags = (SX_FLAG_PLAIN if plain else 0) | {"auto": 0, "device": SX_FLAG_ENV_DEVICE,
+                                                    "host": SX_FLAG_ENV_HOST}[envelopes]
+        o = SxOpts(device, host_threads, flags, pipeline_blocks, batch_bytes)
         h = C.c_void_p()
         _check(lib.sx_create(C.byref(o), C.byref(h)))
         self.h = h

@@ -363,6 +363,28 @@ def test_pipeline_blocks_same_hits():
             e.close()
 
 
+@pytest.mark.parametrize("where", ["device", "host"])
+def test_envelope_rescoring_device_and_host(where):
+    """Envelope rescoring (full-matrix Forward/Backward, posterior, null2,
+    optimal-accuracy coordinates) forced onto the device or the host: both
+    give the oracle's hits, domains and coordinates, filters on and off."""
+    e = sxhmm.Engine(envelopes=where)
+    try:
+        _cmp(e, fixture_text(), fixture_targets(), filters=False)
+        _cmp(e, fixture_text(), fixture_targets(), filters=True)
+        w = small_config(0, 0.2)
+        seqs = [(w.target_ids[i], "".join("ACDEFGHIKLMNPQRSTVWY"[x] for x in s)) for i, s in enumerate(w.targets)]
+        _cmp(e, w.hmm_text(), seqs, filters=True)
+        w = small_config(1, 0.01)
+        seqs = [(w.target_ids[i], "".join("ACDEFGHIKLMNPQRSTVWY"[x] for x in s)) for i, s in enumerate(w.targets)]
+        _cmp(e, w.hmm_text(), seqs, filters=True)
+        _cmp(e, tiny_text() + small_profiles_text(), edge_targets(), cutoff="T", seq=-1e9, dom=-1e9, filters=False)
+        st = e.stats()
+        assert (st["pairs_out"][5] > 0) == (where == "device")
+    finally:
+        e.close()
+
+
 def test_forward_error_vs_fp64_logspace(engine):
     """FP32 odds-space Forward with per-row scaling (bit-identical to the
     reference) against an FP64 log-space Forward: within 0.01 bits."""

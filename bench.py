@@ -259,13 +259,16 @@ def adjoint_run(sxhmm, eng, torch):
         torch.cuda.synchronize()
         ms.append((time.perf_counter() - t0) * 1e3)
     # homolog-heavy search on the same data (hmmsearch --max: every one of the
-    # 16 x 4,096 pairs reaches domain definition): envelope rescoring on the
-    # device (the engine's choice here) against the host
-    # (the adjoint profiles carry no STATS, so a bit-score cutoff reports the hits)
+    # 16 x 4,096 pairs reaches domain definition): envelope rescoring and the
+    # stochastic traces of multi-domain regions on the device, envelopes on
+    # the device with traces on the host, the engine's own choice, and all on
+    # the host (the adjoint profiles carry no STATS, so a bit-score cutoff
+    # reports the hits)
     cfg_max = sxhmm.SearchConfig(sxhmm.Cutoff.bits(0.0, 0.0), sxhmm.PipelineConfig(filters=False)).to_c()
     dom = {}
-    for where in ("device", "host"):
-        e2 = sxhmm.Engine(device=torch.cuda.current_device(), envelopes=where)
+    for where, envelopes, traces in (("device", "device", "device"), ("device_host_traces", "device", "host"),
+                                     ("auto", "auto", "auto"), ("host", "host", "auto")):
+        e2 = sxhmm.Engine(device=torch.cuda.current_device(), envelopes=envelopes, traces=traces)
         ps2 = e2.load_text(text, source="adjoint")
         ts2 = e2.targets_digital(seq, offs, lens)
         e2.search(ps2, ts2, cfg_max)  # warm-up
@@ -273,8 +276,11 @@ def adjoint_run(sxhmm, eng, torch):
         t0 = time.perf_counter()
         hits, doms = e2.search(ps2, ts2, cfg_max)
         torch.cuda.synchronize()
+        st = e2.stats()
         dom[where] = {"ms": round((time.perf_counter() - t0) * 1e3, 1), "hits": len(hits), "domains": len(doms),
-                      "envelopes_on_device": e2.stats()["pairs_out"][5]}
+                      "envelopes_on_device": st["pairs_out"][5], "regions_traced_on_device": st["pairs_out"][6],
+                      "regions_redone_on_host": st["pairs_in"][6] - st["pairs_out"][6],
+                      "host_busy_ms": round(st["ms"][5], 1), "host_tail_ms": round(st["ms"][7], 1)}
         ps2.close()
         ts2.close()
         e2.close()

@@ -47,6 +47,13 @@ extern "C" {
  * device cascade).  Results are identical either way. */
 #define SX_FLAG_ENV_DEVICE 2u /* always on the device */
 #define SX_FLAG_ENV_HOST 4u   /* always on the host */
+/* Where the stochastic-trace ensembles of multi-domain regions (200 sampled
+ * traces each, region_trace_ensemble) run when a block's envelopes go to the
+ * device (default: chosen per profile block; the device when the block's
+ * regions would cost the host pool more than one device trace pass takes).
+ * Results are identical either way. */
+#define SX_FLAG_TRACE_HOST 8u    /* always on the host */
+#define SX_FLAG_TRACE_DEVICE 16u /* always on the device (with the envelopes) */
 
 typedef struct sx_engine sx_engine;
 typedef struct sx_profiles sx_profiles;
@@ -196,7 +203,10 @@ void sx_hits_free(sx_hits* h);
  * 5 domain definition (busy time of the host pool, which overlaps the
  * device stages of later profile blocks), 6 whole call (host clock), 7 host
  * time after the last device work (the part of stage 5 not hidden).
- * pairs_out[5] counts the envelopes rescored by the device passes. */
+ * pairs_out[5] counts the envelopes rescored by the device passes.
+ * Slot 6: stochastic-trace ensembles of multi-domain regions on the device:
+ * pairs_in[6] regions sent, pairs_out[6] regions the device completed (the
+ * rest are redone on the host), cells[6] DP cells of their Forward matrices. */
 typedef struct {
   int64_t pairs_in[8], pairs_out[8];
   double cells[8];

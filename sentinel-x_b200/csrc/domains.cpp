@@ -91,6 +91,7 @@ class Lcg {
     x_ = x_ * 69069u + 1u;
     return (double)x_ / 4294967296.0;
   }
+  uint32_t state() const { return x_; }
 
  private:
   uint32_t seed_, x_ = 0;
@@ -770,6 +771,7 @@ class EnvelopeScorer {
     return std::llabs((a.j - a.m) - (b.j - b.m)) <= 4;
   }
 
+ public:
   static std::vector<std::pair<int64_t, int64_t>> cluster(const std::vector<Sample>& sp, int nsamples) {
     const size_t n = sp.size();
     // esl_cluster_SingleLinkage traversal (pipeline.rs:330-355)
@@ -835,6 +837,7 @@ class EnvelopeScorer {
     return out;
   }
 
+ private:
   // Leftmost (left=true) or rightmost endpoint whose count reaches thr, else
   // the most frequent one (pipeline.rs:489-525).
   static int64_t endpoint(const std::vector<int64_t>& v, size_t thr, bool left) {
@@ -1065,6 +1068,7 @@ struct DomainBatch::Impl {
     bool null2_done;
     bool pass;         // false: rescore rejects the envelope before any pass
     int64_t req = -1;  // index into reqs
+    int32_t region = -1;  // >= 0: placeholder for the envelopes of this region's trace ensemble
   };
   struct PairState {
     bool begun = false;
@@ -1076,9 +1080,13 @@ struct DomainBatch::Impl {
     int64_t nregions = 0;
     std::vector<float> n2sc;
     std::vector<Pending> pend;
+    std::vector<std::pair<int64_t, int64_t>> regions;                   // multi-domain regions left to the device
+    std::vector<std::vector<std::pair<int64_t, int64_t>>> region_envs;  // their clustered envelopes
   };
   SearchOpts o;
   std::vector<PairState> pairs;
+  std::vector<RegionRequest> regs;
+  bool regs_built = false;
   std::vector<EnvRequest> reqs;
 };
 
@@ -1089,7 +1097,7 @@ DomainBatch::DomainBatch(const SearchOpts& o, size_t npairs) : impl_(new Impl) {
 DomainBatch::~DomainBatch() = default;
 
 void DomainBatch::begin(size_t q, const ProfileHost& p, int32_t pi, const uint8_t* dsq, int64_t l, int32_t ti,
-                        const RawRows& rows, float fwdsc) {
+                        const RawRows& rows, float fwdsc, bool device_regions) {
   Impl::PairState& st = impl_->pairs[q];
   st.p = &p;
   st.dsq = dsq;
@@ -1104,7 +1112,10 @@ void DomainBatch::begin(size_t q, const ProfileHost& p, int32_t pi, const uint8_
   };
   st.begun = decode_regions(p, l, rows, fwdsc, st.nexpected, [&](int64_t ri, int64_t j, bool multi) {
     st.nregions++;
-    if (multi) {  // stochastic traces and clustering stay on the host; their envelopes are batched
+    if (multi && device_regions) {  // traced on the device; expand() fills in the envelopes
+      st.pend.push_back({ri, j, true, true, -1, (int32_t)st.regions.size()});
+      st.regions.emplace_back(ri, j);
+    } else if (multi) {  // stochastic traces and clustering here; their envelopes are batched
       for (auto [ei, ej] : es.trace_ensemble(ri, j, st.n2sc)) add(ei, ej, true);
     } else {
       add(ri, j, false);
@@ -1112,12 +1123,63 @@ void DomainBatch::begin(size_t q, const ProfileHost& p, int32_t pi, const uint8_
   });
 }
 
+const std::vector<RegionRequest>& DomainBatch::regions() {
+  Impl& I = *impl_;
+  if (I.regs_built) return I.regs;
+  I.regs_built = true;
+  for (size_t q = 0; q < I.pairs.size(); q++) {
+    Impl::PairState& st = I.pairs[q];
+    if (!st.begun || st.regions.empty()) continue;
+    st.region_envs.assign(st.regions.size(), {});
+    const SpecialTr multi = special_transitions(st.l, true);
+    for (size_t r = 0; r < st.regions.size(); r++)
+      I.regs.push_back({(int32_t)q, st.pi, st.ti, st.regions[r].first, st.regions[r].second, multi, (int32_t)r});
+  }
+  return I.regs;
+}
+
+// The rest of region_trace_ensemble (src/hmmer/pipeline.rs:360-477) after the
+// device's traces: the position-specific null2 from the per-position sums,
+// then single-linkage clustering of the sampled domains.
+void DomainBatch::expand(size_t r, const std::vector<TraceSample>& samples, const float* n2sum, bool ok) {
+  Impl& I = *impl_;
+  const RegionRequest& g = I.regs[r];
+  Impl::PairState& st = I.pairs[(size_t)g.pair];
+  auto& envs = st.region_envs[(size_t)g.local];
+  if (!ok) {
+    EnvelopeScorer es(*st.p, st.dsq, st.l, I.o);
+    envs = es.trace_ensemble(g.i, g.j, st.n2sc);
+    return;
+  }
+  constexpr int kSamples = 200;
+  for (int64_t v = g.i; v <= g.j; v++) st.n2sc[(size_t)v] = std::log(n2sum[v - g.i + 1] / (float)kSamples);
+  std::vector<Sample> sp(samples.size());
+  for (size_t x = 0; x < samples.size(); x++)
+    sp[x] = {(size_t)samples[x].trace, samples[x].i, samples[x].j, samples[x].k, samples[x].m};
+  envs = EnvelopeScorer::cluster(sp, kSamples);
+}
+
+uint32_t DomainBatch::trace_lcg_start() { return Lcg(42).state(); }
+
 const std::vector<EnvRequest>& DomainBatch::requests() {
   Impl& I = *impl_;
   I.reqs.clear();
   for (size_t q = 0; q < I.pairs.size(); q++) {
     Impl::PairState& st = I.pairs[q];
     if (!st.begun) continue;
+    if (!st.regions.empty()) {  // each region placeholder becomes its envelopes, in order
+      std::vector<Impl::Pending> flat;
+      for (const Impl::Pending& e : st.pend) {
+        if (e.region < 0) {
+          flat.push_back(e);
+          continue;
+        }
+        for (auto [ei, ej] : st.region_envs[(size_t)e.region])
+          flat.push_back({ei, ej, true, !(ei == 0 || ej < ei || ej > st.l), -1, -1});
+      }
+      st.pend.swap(flat);
+      st.regions.clear();
+    }
     const SpecialTr uni = special_transitions(st.l, false);
     for (Impl::Pending& e : st.pend) {
       if (!e.pass) continue;

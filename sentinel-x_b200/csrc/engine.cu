@@ -213,22 +213,24 @@ typedef void (*EnvPostFn)(const sxk::EnvRec*, int, const DevProfile*, const floa
                           float*);
 template <int I>
 struct EnvTable {
-  static void fill(EnvPassFn* f, EnvPassFn* b, EnvPostFn* p) {
+  static void fill(EnvPassFn* f, EnvPassFn* b, EnvPostFn* p, EnvPassFn* rf) {
     f[I] = sxk::env_forward_kernel<kVcBins[I]>;
     b[I] = sxk::env_backward_kernel<kVcBins[I]>;
     p[I] = sxk::env_post_kernel<kVcBins[I]>;
-    EnvTable<I + 1>::fill(f, b, p);
+    rf[I] = sxk::env_forward_kernel<kVcBins[I], true>;
+    EnvTable<I + 1>::fill(f, b, p, rf);
   }
 };
 template <>
 struct EnvTable<kNumVbins> {
-  static void fill(EnvPassFn*, EnvPassFn*, EnvPostFn*) {}
+  static void fill(EnvPassFn*, EnvPassFn*, EnvPostFn*, EnvPassFn*) {}
 };
 
 struct KernelTables {
   MsvFn msv[kNumMsvShapes];
   EnvPassFn envf[kNumVbins], envb[kNumVbins];
   EnvPostFn envp[kNumVbins];
+  EnvPassFn regf[kNumVbins];
   VitFn vit[kNumVbins];
   FwdFn fwd[kNumVbins];
   BwdFn bwd[kNumVbins];
@@ -239,7 +241,7 @@ struct KernelTables {
     MsvTable<0>::fill(msv);
     VitGTable<0>::fill(vitg);
     VbinTable<0>::fill(vit, fwd, bwd, adjf, adjb);
-    EnvTable<0>::fill(envf, envb, envp);
+    EnvTable<0>::fill(envf, envb, envp, regf);
   }
 };
 const KernelTables& kernels() {
@@ -508,6 +510,9 @@ struct sx_engine {
   DevBuf<sxk::EnvRec> env_recs;
   DevBuf<float> env_planes, env_rows, env_aux, env_out;
   DevBuf<double> env_fac;
+  DevBuf<sxk::TraceRec> trc_recs;  // stochastic-trace passes of multi-domain regions
+  DevBuf<int32_t> trc_pool, trc_count, trc_status;
+  DevBuf<float> trc_cols;
   DevBuf<Thresholds> thr;
   DevBuf<float> rows_f, rows_b;
   DevBuf<int64_t> row_off;
@@ -1371,6 +1376,169 @@ int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T,
   return launches;
 }
 
+// The device passes of the stochastic traces of multi-domain regions: the
+// region's multihit Forward matrix (M, I and D planes in the diagonal
+// layout), then one warp per region samples the trace ensemble and sums the
+// per-position null2; the samples come back compacted into one pool.  The host finishes each region
+// (logs, clustering) with DomainBatch::expand, and redoes on its own any
+// region the device flagged.  Runs after the cascade, like envelope_passes.
+struct RegionSource {
+  DomainBatch* db;
+  const std::vector<RegionRequest>* regs;
+};
+struct RegionPassStats {
+  int64_t launches = 0, device = 0, redone = 0;
+  double cells = 0;
+};
+
+RegionPassStats region_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T,
+                              std::vector<RegionSource>& srcs, int nthr) {
+  RegionPassStats st;
+  std::vector<std::pair<uint32_t, uint32_t>> items;
+  for (size_t b = 0; b < srcs.size(); b++)
+    for (size_t r = 0; r < srcs[b].regs->size(); r++) items.emplace_back((uint32_t)b, (uint32_t)r);
+  const size_t nr = items.size();
+  if (!nr) return st;
+  auto reg = [&](size_t x) -> const RegionRequest& { return (*srcs[items[x].first].regs)[items[x].second]; };
+  sxk::TraceConsts tc{};
+  tc.lcg0 = DomainBatch::trace_lcg_start();
+  for (int d = 0; d < 4; d++) {
+    const Degenerate& g = degenerate(20 + d);
+    tc.deg_n[d] = g.n;
+    for (int q = 0; q < g.n; q++) tc.deg_m[d][q] = (int8_t)g.members[q];
+  }
+  const auto& K = kernels();
+  cudaStream_t s = E->env_stream;
+  // a batch is one latency-bound wave of 200-trace chains: keep the batches few
+  const int64_t budget = std::max<int64_t>(E->batch_bytes * 2, 1LL << 30);
+  constexpr int64_t kPoolPerRegion = 1024;
+  // column tables of the profiles that have regions (exact copies of the host's
+  // probabilities and match odds), uploaded once
+  std::unordered_map<int32_t, int64_t> col_of;
+  std::vector<float> hcols;
+  for (size_t x = 0; x < nr; x++) {
+    const int32_t p = reg(x).p;
+    if (col_of.count(p)) continue;
+    const ProfileHost& h = P->h[p];
+    col_of[p] = (int64_t)hcols.size();
+    for (int k = 1; k <= h.m; k++) {
+      const float c[8] = {h.p[TBM][k], h.p[TMM][k - 1], h.p[TIM][k - 1], h.p[TDM][k - 1],
+                          h.p[TMI][k],  h.p[TII][k],     h.p[TMD][k - 1], h.p[TDD][k - 1]};
+      hcols.insert(hcols.end(), c, c + 8);
+      for (int x2 = 0; x2 < sxk::kTraceRes; x2++) hcols.push_back(h.mo_row(x2)[k]);
+    }
+  }
+  E->trc_cols.upload(hcols.data(), hcols.size(), s);  // sampled domains per region, on average, before regions are redone
+  std::vector<size_t> order(nr);
+  std::iota(order.begin(), order.end(), (size_t)0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](size_t x, size_t y) { return P->dp[reg(x).p].vbin < P->dp[reg(y).p].vbin; });
+  size_t a = 0;
+  while (a < nr) {
+    size_t b = a;
+    int64_t planes = 0, rowsz = 0, n2 = 0;
+    std::vector<sxk::EnvRec> frecs;
+    std::vector<sxk::TraceRec> trecs;
+    while (b < nr) {
+      const RegionRequest& g = reg(order[b]);
+      const int64_t lr = g.j - g.i + 1;
+      const int64_t need = 3 * sxk::diag_plane(lr, P->h[g.p].m);
+      if (b > a && (planes + need) * (int64_t)sizeof(float) > budget) break;
+      sxk::EnvRec f{};
+      f.p = g.p;
+      f.t = g.t;
+      f.i0 = (int32_t)(g.i - 1);
+      f.lr = (int32_t)lr;
+      f.ploop = g.st.ploop;
+      f.pmove = g.st.pmove;
+      f.pe_loop = g.st.pe_loop;
+      f.pe_move = g.st.pe_move;
+      f.plane_off = planes;
+      f.row_off = rowsz;
+      sxk::TraceRec t{};
+      t.m = P->h[g.p].m;
+      t.t = f.t;
+      t.i0 = f.i0;
+      t.lr = f.lr;
+      t.ploop = f.ploop;
+      t.pmove = f.pmove;
+      t.pe_loop = f.pe_loop;
+      t.pe_move = f.pe_move;
+      t.plane_off = planes;
+      t.row_off = rowsz;
+      t.n2_off = n2;
+      t.col_off = col_of[g.p];
+      planes += need;
+      rowsz += 6 * (lr + 1);
+      n2 += lr + 1;
+      st.cells += (double)P->h[g.p].m * (double)lr;
+      frecs.push_back(f);
+      trecs.push_back(t);
+      b++;
+    }
+    const size_t n = b - a;
+    const int64_t pool_cap = std::min<int64_t>((int64_t)n * kPoolPerRegion, INT32_MAX / sxk::kTraceRecord);
+    E->env_recs.upload(frecs.data(), n, s);
+    E->trc_recs.upload(trecs.data(), n, s);
+    E->env_planes.alloc((size_t)planes);
+    E->env_rows.alloc((size_t)rowsz);
+    E->env_aux.alloc((size_t)n2);
+    E->trc_pool.alloc((size_t)pool_cap * sxk::kTraceRecord);
+    E->trc_count.alloc(1);
+    E->trc_status.alloc(n);
+    CK(cudaMemsetAsync(E->trc_count.p, 0, sizeof(int32_t), s));
+    // the region Forward passes, one launch per vbin (regions are sorted by
+    // vbin), then one trace launch over the batch
+    for (size_t x = 0; x < n;) {
+      const int vb = P->dp[reg(order[a + x]).p].vbin;
+      size_t y = x;
+      while (y < n && P->dp[reg(order[a + y]).p].vbin == vb) y++;
+      const int cnt = (int)(y - x);
+      K.regf[vb]<<<(int)std::min<int64_t>(cnt, (int64_t)E->num_sms * 32), 32, 0, s>>>(
+          E->env_recs.p + x, cnt, P->d_prof.p, P->d_vfb.p, T->d_res.p, T->d_off.p, E->env_planes.p, E->env_rows.p);
+      st.launches += 1;
+      x = y;
+    }
+    sxk::env_trace_kernel<<<(int)std::min<int64_t>(((int64_t)n + 3) / 4, (int64_t)E->num_sms * 16), 128, 0, s>>>(
+        E->trc_recs.p, (int)n, E->trc_cols.p, T->d_res.p, T->d_off.p, E->env_planes.p, E->env_rows.p, E->env_aux.p,
+        E->trc_pool.p, E->trc_count.p, (int32_t)pool_cap, 0, E->trc_status.p, tc);
+    st.launches += 1;
+    CK(cudaGetLastError());
+    std::vector<float> hn2((size_t)n2);
+    std::vector<int32_t> hstatus(n);
+    int32_t count = 0;
+    CK(cudaMemcpyAsync(hn2.data(), E->env_aux.p, sizeof(float) * (size_t)n2, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hstatus.data(), E->trc_status.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&count, E->trc_count.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const int64_t used = std::min<int64_t>(count, pool_cap);
+    std::vector<int32_t> hpool((size_t)used * sxk::kTraceRecord);
+    if (used > 0) {
+      CK(cudaMemcpyAsync(hpool.data(), E->trc_pool.p, sizeof(int32_t) * hpool.size(), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+    }
+    // samples per region, in pool order (a warp reserves each trace's block in
+    // trace order, so pool order within a region is trace order)
+    std::vector<std::vector<TraceSample>> per(n);
+    for (int64_t q = 0; q < used; q++) {
+      const int32_t* o = hpool.data() + q * sxk::kTraceRecord;
+      if (o[0] < 0 || (size_t)o[0] >= n) continue;
+      per[(size_t)o[0]].push_back({o[1], (int64_t)o[2], (int64_t)o[3], o[4], o[5]});
+    }
+    std::atomic<int64_t> redone{0};
+    parallel_for(n, nthr, [&](size_t x) {
+      const auto& it = items[order[a + x]];
+      const bool ok = hstatus[x] == 0;
+      if (!ok) redone++;
+      srcs[it.first].db->expand(it.second, per[x], hn2.data() + trecs[x].n2_off, ok);
+    });
+    st.redone += redone.load();
+    st.device += (int64_t)n - redone.load();
+    a = b;
+  }
+  return st;
+}
+
 // Contiguous ranges of profile indices with about equal filtered DP cells.
 // Each range runs through the device cascade as one block; the host domain
 // definition of a block overlaps the device work of the blocks after it.
@@ -1610,6 +1778,7 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     std::vector<EnvRequest> reqs;
     std::vector<EnvFactors> F;
     std::vector<EnvDeviceOut> D;
+    bool dev_regions = false;  // its multi-domain regions wait for the device trace passes
   };
   std::vector<std::unique_ptr<PendingBatch>> pending;  // appended by the pool's driver thread only
   HostQueue hq(E->host_threads);  // declared after what its jobs use, so it is joined first
@@ -1628,6 +1797,25 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     const double host_ms = fin * 44e-9 * 1e3 / std::max(1, E->host_threads);
     const double dev_ms = block_cells / 4.4e12 * 1e3;
     return host_ms > 0.5 * dev_ms + 5.0;
+  };
+  // Stochastic traces of a block's multi-domain regions: on the host pool at
+  // once (hidden behind later device work) unless their estimated host time
+  // exceeds the device trace pass.  Host: ~19 ns per DP cell of a region's
+  // Forward matrix, traces included, per thread.  Device: one warp per region
+  // runs its 200 traces as one dependent chain of ~200 (L + M) steps at
+  // ~0.75 us each (B200), so a pass lasts about one chain per wave of
+  // concurrent regions (20 per SM), plus ~30 ms of copies and host clustering.
+  auto device_traces = [&](const std::vector<RegionRequest>& regs, int nthr) {
+    if (E->flags & SX_FLAG_TRACE_DEVICE) return true;
+    if (E->flags & SX_FLAG_TRACE_HOST) return false;
+    double cells = 0, chain = 0;
+    for (const RegionRequest& g : regs) {
+      const double lr = (double)(g.j - g.i + 1), m = (double)P->h[g.p].m;
+      cells += m * lr;
+      chain = std::max(chain, 200.0 * (lr + m) * 0.75e-3);
+    }
+    const double waves = std::ceil((double)regs.size() / (20.0 * E->num_sms));
+    return cells * 19e-6 / std::max(1, nthr) > 30.0 + waves * chain;
   };
   auto rows_and_queue = [&](Slot& S, BlockOut* B, bool dev_env) {
     B->res.resize(B->finals.size());
@@ -1663,8 +1851,8 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
             });
             return;
           }
-          // F3 (pipeline.rs:179-183), posterior decoding, regions and the
-          // stochastic traces of multi-domain regions on the host; the
+          // F3 (pipeline.rs:179-183), posterior decoding and regions on the
+          // host; the stochastic traces of multi-domain regions and the
           // envelopes' full-matrix passes wait until the cascade is done
           auto pb = std::make_unique<PendingBatch>();
           pb->B = B;
@@ -1685,11 +1873,13 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
                 std::exp(exp_tail_logsurv((double)((fwdsc - f.filtersc) / kLn2f), h.fwd[0], h.fwd[1])) > o.f3)
               return;
             n_domain++;
-            db.begin(q, h, f.p, T->dsq.data() + T->off[f.t], l, f.t, RawRows{fr, br}, fwdsc);
+            db.begin(q, h, f.p, T->dsq.data() + T->off[f.t], l, f.t, RawRows{fr, br}, fwdsc, true);
             begun[q] = 1;
           });
-          pb->reqs = db.requests();
-          n_env += (int64_t)pb->reqs.size();
+          const std::vector<RegionRequest>& regs = db.regions();
+          pb->dev_regions = !regs.empty() && device_traces(regs, nthr);
+          if (!regs.empty() && !pb->dev_regions)
+            parallel_for(regs.size(), nthr, [&](size_t r) { db.expand(r, {}, nullptr, false); });
           pending.push_back(std::move(pb));
         } catch (const CudaError& ce) {
           std::lock_guard<std::mutex> g(host_err_mu);
@@ -1747,10 +1937,21 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
   const auto t_dev = std::chrono::steady_clock::now();
   E->stats.ms[5] = hq.finish();
   if (host_err_code) return fail(host_err_code, host_err_msg);
-  // every envelope of the search through the device passes at once, on an
-  // idle GPU, then each pair's scores
+  // every multi-domain region's trace ensemble, then every envelope of the
+  // search through the device passes at once, on an idle GPU, then each
+  // pair's scores
+  RegionPassStats rstats;
   {
     const auto t_env = std::chrono::steady_clock::now();
+    std::vector<RegionSource> rsrc;
+    for (auto& pb : pending)
+      if (pb->dev_regions) rsrc.push_back({pb->db.get(), &pb->db->regions()});
+    rstats = region_passes(E, P, T, rsrc, E->host_threads);
+    env_launches += rstats.launches;
+    for (auto& pb : pending) {
+      pb->reqs = pb->db->requests();
+      n_env += (int64_t)pb->reqs.size();
+    }
     std::vector<EnvSource> srcs;
     for (auto& pb : pending) srcs.push_back({pb->db.get(), &pb->reqs, &pb->F, &pb->D});
     env_launches += envelope_passes(E, P, T, srcs, E->host_threads);
@@ -1768,6 +1969,9 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
   }
   E->stats.kernel_launches += env_launches.load();
   E->stats.pairs_out[5] = n_env.load();
+  E->stats.pairs_in[6] = rstats.device + rstats.redone;
+  E->stats.pairs_out[6] = rstats.device;
+  E->stats.cells[6] = rstats.cells;
   const auto t_end = std::chrono::steady_clock::now();
   E->stats.pairs_in[4] = nfinal;
   E->stats.pairs_out[4] = n_domain.load();

@@ -43,9 +43,18 @@ __device__ __forceinline__ int64_t plane_at(int64_t row, int k) {
   return row * (32 * VC) + (int64_t)(((k - 1) % VC) * 32 + (k - 1) / VC);
 }
 
+// Diagonal layout of a region's M/I/D planes for the stochastic traceback:
+// cell (i, k), 1 <= i <= lr, 1 <= k <= M, at (i - k + M - 1) * M + (k - 1), so
+// the cells of a run of match states, (i, k) -> (i-1, k-1), are adjacent.
+__host__ __device__ __forceinline__ int64_t diag_at(int64_t i, int k, int M) {
+  return (i - k + M - 1) * (int64_t)M + (k - 1);
+}
+__host__ __device__ __forceinline__ int64_t diag_plane(int64_t lr, int M) { return (lr + M - 1) * (int64_t)M; }
+
 // forward_matrix: M/I planes (scaled, after each row's rescaling) and the raw
-// special rows N B E J C scale for rows 1..lr.
-template <int VC>
+// special rows N B E J C scale for rows 1..lr.  DIAG writes the M, I and D
+// planes in the diagonal layout instead (the stochastic traceback's input).
+template <int VC, bool DIAG = false>
 __global__ void __launch_bounds__(32) env_forward_kernel(const EnvRec* __restrict__ recs, int n,
                                                          const DevProfile* __restrict__ profs,
                                                          const float* __restrict__ vfb,
@@ -65,7 +74,8 @@ __global__ void __launch_bounds__(32) env_forward_kernel(const EnvRec* __restric
     const int L = r.lr;
     const float ploop = r.ploop, pmove = r.pmove, pe_loop = r.pe_loop, pe_move = r.pe_move;
     float* FM = planes + r.plane_off;
-    float* FI = FM + (int64_t)(L + 1) * RS;
+    float* FI = FM + (DIAG ? diag_plane(L, M) : (int64_t)(L + 1) * RS);
+    float* FD = FI + diag_plane(L, M);
     float* orow = rows + r.row_off;
     TransRows<VC> tr;
     tr.load(img, kRowFwd, lane);
@@ -152,8 +162,18 @@ __global__ void __launch_bounds__(32) env_forward_kernel(const EnvRec* __restric
       }
 #pragma unroll
       for (int c = 0; c < VC; c++) {
-        FM[(int64_t)(i + 1) * RS + c * 32 + lane] = mv[c];
-        FI[(int64_t)(i + 1) * RS + c * 32 + lane] = iv[c];
+        if (DIAG) {
+          const int k = lane * VC + c + 1;
+          if (k <= M) {
+            const int64_t at = diag_at(i + 1, k, M);
+            FM[at] = mv[c];
+            FI[at] = iv[c];
+            FD[at] = dv[c];
+          }
+        } else {
+          FM[(int64_t)(i + 1) * RS + c * 32 + lane] = mv[c];
+          FI[(int64_t)(i + 1) * RS + c * 32 + lane] = iv[c];
+        }
         mp[c] = mv[c];
         ip[c] = iv[c];
         dp[c] = dv[c];
@@ -644,6 +664,287 @@ __global__ void __launch_bounds__(32) env_post_kernel(const EnvRec* __restrict__
       out[24] = (float)ck0;
       out[25] = (float)ck1;
     }
+  }
+}
+
+
+// ---- stochastic traceback ensembles of multi-domain regions ------------------
+// region_trace_ensemble (src/hmmer/pipeline.rs:360-477) up to the clustering:
+// kTraceSamples sampled traces (stochastic_trace, src/hmmer/dp.rs:1075-1258)
+// through the region's multihit Forward matrix (env_forward_kernel<VC, true>,
+// diagonal layout), one Easel LCG stream per region, the per-trace null2 of
+// every sampled domain and its per-position sums.  The host clusters the
+// samples and takes the logs.
+
+constexpr int kTraceSamples = 200;
+constexpr int kTraceDoms = 32;   // sampled domains of one trace held in shared memory
+constexpr int kTraceRecord = 6;  // region, trace, sqfrom, sqto, hmmfrom, hmmto (target coordinates)
+constexpr int kTraceRes = 20;    // canonical residues; codes 20..23 degenerate, 24 '*'
+// Per profile column k (1-based), kTraceCol floats at (k-1)*kTraceCol:
+// p_bm[k] p_mm[k-1] p_im[k-1] p_dm[k-1] p_mi[k] p_ii[k] p_md[k-1] p_dd[k-1],
+// then the match odds mo[x][k] of the 20 canonical residues.
+constexpr int kTraceCol = 28;
+
+struct TraceRec {
+  int32_t m, t;        // profile length, target
+  int32_t i0, lr;      // region residues i0 .. i0+lr-1 (0-based)
+  float ploop, pmove;  // multihit special transitions of the target's length
+  float pe_loop, pe_move;
+  int64_t plane_off;   // diagonal M I D planes of env_forward_kernel<VC, true>
+  int64_t row_off;     // its raw special rows, 6 (lr+1)
+  int64_t n2_off;      // per-position null2 sums, lr+1 floats (slot 0 unused)
+  int64_t col_off;     // the profile's column table (kTraceCol floats per column)
+};
+
+struct TraceConsts {
+  uint32_t lcg0;        // LCG state after seeding (esl_mix3 of seed 42)
+  int32_t deg_n[4];     // member counts of the degenerate codes B J Z X
+  int8_t deg_m[4][20];  // their members (esl_abc_FAvgScVec order)
+};
+
+__device__ __forceinline__ double trace_uniform(uint32_t& rng) {
+  rng = rng * 69069u + 1u;
+  return (double)rng * 2.3283064365386962890625e-10;  // / 2^32, exact
+}
+
+// esl_vec_FNorm (Kahan) then esl_rnd_FChoose (src/hmmer/dp.rs:1026-1059); the
+// quotients acc/norm are independent, so all are formed before the first test.
+// The last candidate needs none: with no earlier hit the choice is N-1 whether
+// or not its test passes.
+template <int N>
+__device__ __forceinline__ int trace_choose(uint32_t& rng, float (&v)[N]) {
+  float s = 0.f, comp = 0.f;
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    const float y = __fsub_rn(v[i], comp);
+    const float t = __fadd_rn(s, y);
+    comp = __fsub_rn(__fsub_rn(t, s), y);
+    s = t;
+  }
+#pragma unroll
+  for (int i = 0; i < N; i++) v[i] = s != 0.f ? __fdiv_rn(v[i], s) : 1.f / (float)N;
+  double norm = 0.0, acc[N];
+#pragma unroll
+  for (int i = 0; i < N; i++) norm = __dadd_rn(norm, (double)v[i]);
+  double a = 0.0;
+#pragma unroll
+  for (int i = 0; i < N; i++) acc[i] = a = __dadd_rn(a, (double)v[i]);
+  const double roll = trace_uniform(rng);
+  int pick = N - 1;
+#pragma unroll
+  for (int i = N - 2; i >= 0; i--)
+    if (roll < __ddiv_rn(acc[i], norm)) pick = i;
+  return pick;
+}
+
+// One warp per region; every lane follows the same trace (same loads, same LCG
+// draws), lanes 0..19 carry the null2 sums of the residues, the warp scans the
+// E-state entry candidates 32 at a time (each lane forms the running sum up to
+// its candidate, in order) and all lanes update the per-position sums.  A
+// region that leaves the matrix, or whose samples overflow the pool or the
+// per-trace buffer, is flagged (status 1) for the host to redo.  Pool records
+// carry the region's index `first + w` within the caller's batch.
+__global__ void __launch_bounds__(128) env_trace_kernel(const TraceRec* __restrict__ recs, int n,
+                                                        const float* __restrict__ cols,
+                                                        const uint8_t* __restrict__ res,
+                                                        const int64_t* __restrict__ toff,
+                                                        const float* __restrict__ planes,
+                                                        const float* __restrict__ rows, float* __restrict__ n2sum,
+                                                        int32_t* __restrict__ pool, int32_t* __restrict__ pool_count,
+                                                        int32_t pool_cap, int32_t first, int32_t* __restrict__ status,
+                                                        TraceConsts tc) {
+  __shared__ float sn2[4][32];
+  __shared__ int4 sdom[4][kTraceDoms];
+  const int lane = threadIdx.x & 31;
+  const int wib = (threadIdx.x >> 5) & 3;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  enum { SC, SE, SM, SI, SD, SB, SJ, SN };
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
+    const TraceRec r = recs[w];
+    const int M = r.m;
+    const int L = r.lr;
+    const int64_t PL = diag_plane(L, M);
+    const float* FM = planes + r.plane_off;
+    const float* FI = FM + PL;
+    const float* FD = FI + PL;
+    const float* xr = rows + r.row_off;
+    const float* col = cols + r.col_off;
+    const uint8_t* s = res + toff[r.t] + r.i0;
+    float* ns = n2sum + r.n2_off;
+    bool bad = L < 1 || M < 1;
+    for (int pos = lane; pos <= L; pos += 32) ns[pos] = 0.f;
+    __syncwarp();
+    // planes at (row, k), 1 <= k <= M; row 0 of the matrix is all zero
+    auto plane = [&](const float* X, int row, int k) { return row ? __ldg(X + diag_at(row, k, M)) : 0.f; };
+    auto prob = [&](int q, int k) { return __ldg(col + (k - 1) * kTraceCol + q); };
+    const float pmove = r.pmove, ploop = r.ploop;
+    // special row i, slots N B E J C and the rescale factor (1 when the row was
+    // not rescaled); row 0 is the start state N = 1, B = pmove
+    auto spec = [&](int slot, int i) -> float {
+      if (i == 0) return slot == 0 || slot == 5 ? 1.f : slot == 1 ? pmove : 0.f;
+      const float v = __ldg(xr + 6 * (int64_t)i + slot);
+      return slot == 5 && !(v > 0.f) ? 1.f : v;
+    };
+    const int q_stripes = max(2, (M - 1) / 4 + 1);
+    const int ncand = 8 * q_stripes;
+    // entry candidate c of the E-state scan (the reference's striped order):
+    // stripe c/8, M (c%8 < 4) or D, node (c%4)*q_stripes + c/8 + 1
+    auto cand_k = [&](int c) { return (c & 3) * q_stripes + (c >> 3) + 1; };
+    const int64_t limit = 8 * (int64_t)(L + 2) * (int64_t)(M + 2) + 64;
+    uint32_t rng = tc.lcg0;
+    for (int tr = 0; tr < kTraceSamples && !bad; tr++) {
+      int s0 = SC;
+      int i = L, k = 0;
+      bool have = false;
+      int sqfrom = 0, sqto = 0, hmmfrom = 0, hmmto = 0, nn = 0;
+      float vs = 0.f;  // lane x < 20: sum of mo[x][node] over the domain's nodes
+      int hi = L + 1;  // positions >= hi have their sum for this trace
+      int nd = 0;      // domains of this trace so far (in discovery order: last first)
+      for (int64_t guard = 1; guard <= limit; guard++) {
+        int s1;
+        if (s0 == SC) {
+          if (i == 0) break;
+          float path[2] = {fmul(spec(4, i - 1), ploop), fmul(fmul(spec(2, i), r.pe_move), spec(5, i))};
+          s1 = trace_choose(rng, path) == 0 ? SC : SE;
+        } else if (s0 == SE) {
+          const double roll = trace_uniform(rng);
+          const float norm = (float)__ddiv_rn(1.0, (double)spec(2, i));
+          double acc = 0.0;
+          int pick = 0, pst = SM;
+          for (int pass = 0; pick == 0 && pass < 1000; pass++) {
+            auto load = [&](int c) {
+              const int kk = cand_k(c);
+              return c < ncand && kk <= M ? (double)fmul(plane((c & 4) ? FD : FM, i, kk), norm) : 0.0;
+            };
+            double val = load(lane);
+            for (int c0 = 0; c0 < ncand; c0 += 32) {
+              const double nxt = c0 + 32 < ncand ? load(c0 + 32 + lane) : 0.0;
+              // lane j: the running sum through candidate c0 + j, in order;
+              // a skipped candidate adds +0, which leaves the sum unchanged
+              double run = acc;
+              for (int j = 0; j < 32; j++) {
+                const double v = __shfl_sync(kFull, val, j);
+                if (j <= lane) run = __dadd_rn(run, v);
+              }
+              const unsigned hit = __ballot_sync(kFull, roll < run);
+              if (hit) {
+                const int j = __ffs(hit) - 1;
+                pick = cand_k(c0 + j);
+                pst = ((c0 + j) & 4) ? SD : SM;
+                break;
+              }
+              acc = __shfl_sync(kFull, run, 31);
+              val = nxt;
+            }
+            if (pick == 0 && acc <= 0.0) break;
+          }
+          if (pick == 0) break;
+          k = pick;
+          have = true;
+          sqfrom = sqto = hmmfrom = hmmto = nn = 0;
+          vs = 0.f;
+          s1 = pst;
+        } else if (s0 == SM) {
+          if (i < 1 || k < 1 || k > M) { bad = true; break; }
+          if (have) {
+            if (sqto == 0) { sqto = i; hmmto = k; }
+            sqfrom = i;
+            hmmfrom = k;
+            nn++;
+            if (lane < kTraceRes) vs = __fadd_rn(vs, prob(8 + lane, k));
+          }
+          float path[4] = {fmul(spec(1, i - 1), prob(0, k)), 0.f, 0.f, 0.f};
+          if (k >= 2) {
+            path[1] = fmul(plane(FM, i - 1, k - 1), prob(1, k));
+            path[2] = fmul(plane(FI, i - 1, k - 1), prob(2, k));
+            path[3] = fmul(plane(FD, i - 1, k - 1), prob(3, k));
+          }
+          const int c = trace_choose(rng, path);
+          k -= 1;
+          i -= 1;
+          s1 = c == 0 ? SB : c == 1 ? SM : c == 2 ? SI : SD;
+        } else if (s0 == SD) {
+          float path[2] = {0.f, 0.f};
+          if (k >= 2) {
+            if (k > M) { bad = true; break; }
+            path[0] = fmul(plane(FM, i, k - 1), prob(6, k));
+            path[1] = fmul(plane(FD, i, k - 1), prob(7, k));
+          }
+          const int c = trace_choose(rng, path);
+          k -= 1;
+          s1 = c == 0 ? SM : SD;
+        } else if (s0 == SI) {
+          if (i < 1 || k < 1 || k > M) { bad = true; break; }
+          if (have) {
+            nn++;
+            if (lane < kTraceRes) vs = __fadd_rn(vs, prob(8 + lane, k));
+          }
+          float path[2] = {fmul(plane(FM, i - 1, k), prob(4, k)), fmul(plane(FI, i - 1, k), prob(5, k))};
+          const int c = trace_choose(rng, path);
+          i -= 1;
+          s1 = c == 0 ? SM : SI;
+        } else if (s0 == SB) {
+          if (have) {  // a sampled domain is complete: its null2 and its positions' sums
+            if (nd >= kTraceDoms) { bad = true; break; }
+            const float ld = (float)max(nn, 1);
+            if (lane < kTraceRes) sn2[wib][lane] = __fdiv_rn(vs, ld);
+            __syncwarp();
+            if (lane >= kTraceRes && lane < kTraceRes + 4) {
+              const int d = lane - kTraceRes;
+              float a = 0.f;
+              for (int q = 0; q < tc.deg_n[d]; q++) a = __fadd_rn(a, sn2[wib][tc.deg_m[d][q]]);
+              sn2[wib][lane] = __fdiv_rn(a, (float)tc.deg_n[d]);
+            } else if (lane == kTraceRes + 4) {
+              sn2[wib][lane] = 1.f;
+            }
+            __syncwarp();
+            for (int pos = sqto + 1 + lane; pos < hi; pos += 32) ns[pos] = __fadd_rn(ns[pos], 1.f);
+            for (int pos = sqfrom + 1 + lane; pos <= sqto; pos += 32)
+              ns[pos] = __fadd_rn(ns[pos], sn2[wib][__ldg(s + pos - 1)]);
+            __syncwarp();
+            hi = sqfrom + 1;
+            if (lane == 0) sdom[wib][nd] = make_int4(sqfrom, sqto, hmmfrom, hmmto);
+            nd++;
+            have = false;
+          }
+          float path[2] = {fmul(spec(0, i), pmove), fmul(spec(3, i), pmove)};
+          s1 = trace_choose(rng, path) == 0 ? SN : SJ;
+        } else if (s0 == SJ) {
+          if (i == 0) break;
+          float path[2] = {fmul(spec(3, i - 1), ploop), fmul(fmul(spec(2, i), r.pe_loop), spec(5, i))};
+          s1 = trace_choose(rng, path) == 0 ? SJ : SE;
+        } else {
+          if (i == 0) break;
+          s1 = SN;
+        }
+        if ((s1 == SN || s1 == SJ || s1 == SC) && s1 == s0) i -= 1;
+        s0 = s1;
+      }
+      if (bad) break;
+      for (int pos = 1 + lane; pos < hi; pos += 32) ns[pos] = __fadd_rn(ns[pos], 1.f);
+      __syncwarp();
+      // this trace's domains in sequence order, as one block of the pool
+      int base = 0;
+      if (lane == 0 && nd > 0) base = atomicAdd(pool_count, nd);
+      base = __shfl_sync(kFull, base, 0);
+      if (nd > 0 && (int64_t)base + nd > (int64_t)pool_cap) {  // mark the reserved slots that exist as unused
+        for (int q = lane; q < nd && base + q < pool_cap; q += 32) pool[(int64_t)(base + q) * kTraceRecord] = -1;
+        bad = true;
+        break;
+      }
+      for (int q = lane; q < nd; q += 32) {
+        const int4 d = sdom[wib][nd - 1 - q];
+        int32_t* o = pool + (int64_t)(base + q) * kTraceRecord;
+        o[0] = first + w;
+        o[1] = tr;
+        o[2] = d.x + r.i0;
+        o[3] = d.y + r.i0;
+        o[4] = d.z;
+        o[5] = d.w;
+      }
+      __syncwarp();
+    }
+    if (lane == 0) status[w] = bad ? 1 : 0;
   }
 }
 

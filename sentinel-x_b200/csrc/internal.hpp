@@ -109,10 +109,12 @@ float forward_score_from_rows(const ProfileHost& p, int64_t l, const float* fwd_
 float backward_score_from_rows(int64_t l, const float* bwd_rows);
 // Batched domain definition: the same results as define_domains, with the
 // full-matrix envelope passes of every pair of a batch done elsewhere (on
-// the device).  Phases: begin() per pair (decoding, regions, stochastic-trace
-// clustering on the host) -> requests() -> the caller runs the Forward and
-// Backward envelope passes -> factors() per request -> the caller runs the
-// posterior / null2 / optimal-accuracy pass -> finish() per pair.
+// the device).  Phases: begin() per pair (decoding, regions; the stochastic
+// traces of multi-domain regions either here or, with device_regions, by the
+// caller: regions() -> device trace passes -> expand() per region, which
+// clusters the samples on the host) -> requests() -> the caller runs the
+// Forward and Backward envelope passes -> factors() per request -> the caller
+// runs the posterior / null2 / optimal-accuracy pass -> finish() per pair.
 struct EnvRequest {
   int32_t pair;     // index of the pair in the batch
   int32_t p, t;     // profile and target indices
@@ -133,12 +135,34 @@ struct EnvDeviceOut {
   bool found;     // optimal-accuracy traceback found a domain
   int32_t i0, i1, k0, k1;
 };
+// A multi-domain region whose stochastic traces run on the device.
+struct RegionRequest {
+  int32_t pair;   // index of the pair in the batch
+  int32_t p, t;   // profile and target indices
+  int64_t i, j;   // region, 1-based residues of the target
+  SpecialTr st;   // multihit special transitions of the target's length
+  int32_t local;  // the region's number within its pair
+};
+// One sampled domain of a region's trace ensemble (p7_spcoord_s), target coordinates.
+struct TraceSample {
+  int32_t trace;
+  int64_t i, j;
+  int32_t k, m;
+};
 class DomainBatch {
  public:
   DomainBatch(const SearchOpts& o, size_t npairs);
   ~DomainBatch();
+  // device_regions: the stochastic traces of multi-domain regions are left to
+  // the caller (regions() -> device passes -> expand()); otherwise they run here.
   void begin(size_t q, const ProfileHost& p, int32_t pi, const uint8_t* dsq, int64_t l, int32_t ti,
-             const RawRows& rows, float fwdsc);
+             const RawRows& rows, float fwdsc, bool device_regions = false);
+  const std::vector<RegionRequest>& regions();  // built on the first call, after every begin()
+  // Region r's trace ensemble: its samples in trace order and the per-position
+  // null2 sums (positions 1..lr); ok = false redoes the ensemble on the host.
+  void expand(size_t r, const std::vector<TraceSample>& samples, const float* n2sum, bool ok);
+  // LCG state the device trace streams start from (seed 42 through esl_mix3).
+  static uint32_t trace_lcg_start();
   const std::vector<EnvRequest>& requests();
   void factors(size_t r, const float* fwd_rows, const float* bwd_rows, EnvFactors& f) const;
   bool finish(size_t q, const std::vector<EnvFactors>& f, const std::vector<EnvDeviceOut>& d, HitOut& out);

@@ -12,6 +12,8 @@ SX_CUT_EVALUE, SX_CUT_BITS, SX_CUT_GA, SX_CUT_NC, SX_CUT_TC = range(5)
 SX_FLAG_PLAIN = 1
 SX_FLAG_ENV_DEVICE = 2
 SX_FLAG_ENV_HOST = 4
+SX_FLAG_TRACE_HOST = 8
+SX_FLAG_TRACE_DEVICE = 16
 
 # Every entry point declared in include/sxhmm.h, name -> (restype, argtypes).
 _P = C.c_void_p
@@ -147,10 +149,12 @@ def _ptr(a, t):
 class Engine:
     """One engine per device (sx_create)."""
 
-    def __init__(self, device=0, host_threads=0, plain=False, batch_bytes=0, pipeline_blocks=0, envelopes="auto"):
+    def __init__(self, device=0, host_threads=0, plain=False, batch_bytes=0, pipeline_blocks=0, envelopes="auto",
+                 traces="auto"):
         lib = load_library()
         flags = (SX_FLAG_PLAIN if plain else 0) | {"auto": 0, "device": SX_FLAG_ENV_DEVICE,
                                                     "host": SX_FLAG_ENV_HOST}[envelopes]
+        flags |= {"auto": 0, "device": SX_FLAG_TRACE_DEVICE, "host": SX_FLAG_TRACE_HOST}[traces]
         o = SxOpts(device, host_threads, flags, pipeline_blocks, batch_bytes)
         h = C.c_void_p()
         _check(lib.sx_create(C.byref(o), C.byref(h)))

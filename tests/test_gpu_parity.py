@@ -385,6 +385,28 @@ def test_envelope_rescoring_device_and_host(where):
         e.close()
 
 
+@pytest.mark.parametrize("traces", ["device", "host"])
+def test_stochastic_traces_device_and_host(traces):
+    """Multi-domain regions of homolog-heavy targets (0-3 planted domains per
+    target, M = 300): their 200-trace ensembles sampled on the device (region
+    Forward matrix, traces, per-position null2 sums; clustering on the host)
+    or on the host give the oracle's hits, domains and coordinates."""
+    from sxhmm import synth
+    w = synth.make_config(3, scale=1 / 8)
+    seqs = [(w.target_ids[i], "".join("ACDEFGHIKLMNPQRSTVWY"[x] for x in s)) for i, s in enumerate(w.targets)]
+    e = sxhmm.Engine(envelopes="device", traces=traces)
+    try:
+        _cmp(e, w.hmm_text(), seqs, cutoff="T", seq=0.0, dom=0.0, filters=False)
+        st = e.stats()
+        if traces == "device":
+            assert st["pairs_out"][6] > 0 and st["pairs_in"][6] == st["pairs_out"][6], st
+            assert st["cells"][6] > 0
+        else:
+            assert st["pairs_in"][6] == 0
+    finally:
+        e.close()
+
+
 def test_forward_error_vs_fp64_logspace(engine):
     """FP32 odds-space Forward with per-row scaling (bit-identical to the
     reference) against an FP64 log-space Forward: within 0.01 bits."""

@@ -502,6 +502,7 @@ struct sx_engine {
   std::mutex mu;
   sx_search_stats stats{};
   int pipeline_blocks = 0;  // profile blocks per search; 0 = by workload size
+  int64_t mem_free = 0;     // device memory free when the engine was created
   BlockPool target_blocks;  // device memory of freed target sets
   // envelope passes of the host domain definition (used by the host pool's
   // driver thread, one batch at a time)
@@ -882,6 +883,25 @@ struct RowsChunk {
   std::vector<size_t> which;  // pair q's index in the caller's list
 };
 
+// Device memory free when the engine was created (0 = unknown).  Queried once:
+// with the query at the start of every search, a stream of end-to-end
+// searches ran tens of milliseconds slower per call.
+void note_free_memory(sx_engine* E) {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    fr = 0;
+  }
+  E->mem_free = (int64_t)fr;
+}
+// Bytes a pass may take for its scratch: the configured budget, capped by half
+// of the device memory that was free when the engine was created (other
+// processes on the GPU, other engines), and never below 64 MB.
+int64_t scratch_budget(const sx_engine* E, int64_t want) {
+  if (E->mem_free <= 0) return want;
+  return std::max<int64_t>(std::min<int64_t>(want, E->mem_free / 2), 64LL << 20);
+}
+
 // Device Forward and Backward with row output for `pairs`, in chunks bounded
 // by `row_budget` floats per direction; hands each chunk's host copy to
 // consume(RowsChunk&&) as soon as it has arrived.
@@ -890,7 +910,7 @@ void rows_pass(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T,
                Consume&& consume) {
   if (pairs.empty()) return;
   const auto& K = kernels();
-  const int64_t row_budget = std::max<int64_t>(E->batch_bytes / 2 / (int64_t)sizeof(float), 1 << 20);
+  const int64_t row_budget = std::max<int64_t>(scratch_budget(E, E->batch_bytes / 2) / (int64_t)sizeof(float), 1 << 20);
   size_t i0 = 0;
   while (i0 < pairs.size()) {
     // chunk [i0, i1)
@@ -1259,7 +1279,7 @@ int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T,
   auto out_of = [&](size_t x) -> EnvDeviceOut& { return (*srcs[items[x].first].D)[items[x].second]; };
   const auto& K = kernels();
   cudaStream_t s = E->env_stream;
-  const int64_t budget = std::max<int64_t>(E->batch_bytes / 2, 256LL << 20);
+  const int64_t budget = scratch_budget(E, std::max<int64_t>(E->batch_bytes / 2, 256LL << 20));
   std::vector<size_t> order(nr);
   std::iota(order.begin(), order.end(), (size_t)0);
   std::stable_sort(order.begin(), order.end(),
@@ -1410,7 +1430,7 @@ RegionPassStats region_passes(sx_engine* E, const sx_profiles* P, const sx_targe
   const auto& K = kernels();
   cudaStream_t s = E->env_stream;
   // a batch is one latency-bound wave of 200-trace chains: keep the batches few
-  const int64_t budget = std::max<int64_t>(E->batch_bytes * 2, 1LL << 30);
+  const int64_t budget = scratch_budget(E, std::max<int64_t>(E->batch_bytes * 2, 1LL << 30));
   constexpr int64_t kPoolPerRegion = 1024;
   // column tables of the profiles that have regions (exact copies of the host's
   // probabilities and match odds), uploaded once
@@ -2026,6 +2046,7 @@ int sx_create(const sx_opts* opts, sx_engine** out) {
       CK(cudaStreamCreateWithPriority(&e->env_stream2, cudaStreamNonBlocking, greatest));
       CK(cudaEventCreateWithFlags(&e->env_ev, cudaEventDisableTiming));
     }
+    note_free_memory(e.get());
     (void)kernels();
   } catch (const CudaError& ce) {
     return fail(ce.code, ce.msg);
@@ -2471,7 +2492,7 @@ int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, c
     cudaStream_t s = e->stream;
     const int vb = p->dp[pair_profile[0]].vbin, VC = kVcBins[vb];
     const auto& K = kernels();
-    const int64_t budget = std::max<int64_t>(e->batch_bytes, 64LL << 20);
+    const int64_t budget = scratch_budget(e, std::max<int64_t>(e->batch_bytes, 64LL << 20));
     size_t i0 = 0;
     while (i0 < npairs) {
       // chunk: scratch floats per pair ~ (L/S + S + 2) * 3 * 32 * VC + 6 (L+1) + out, doubles (L+1)

@@ -163,6 +163,36 @@ def test_search_unit_known_answers(engine):
     assert len(b) == 1 and b[0][1] == 0 and b[0][6][0][8]
 
 
+def _decode(x):
+    return "".join("ACDEFGHIKLMNPQRSTVWY"[c] for c in x)
+
+
+def test_search_marker_set_gathering(engine):
+    """Marker-set shape (BUSCO/EukCC-like, shrunk): markers of M 200-1500
+    planted once in most genomes; one search per genome with the profiles'
+    gathering cutoffs (Cutoff::Gathering), filters on."""
+    w = small_config(2, 0.02)
+    text = w.hmm_text()
+    ps = engine.load_text(text)
+    total = 0
+    for g0, n in w.truth["genomes"]:
+        seqs = [(w.target_ids[i], _decode(w.targets[i])) for i in range(g0, g0 + n)]
+        a = _hits_oracle(text, seqs, O.make_cfg(cutoff="GA", seq=0.0, dom=0.0))
+        b = _hits_gpu(engine, text, seqs, {"cutoff": "GA"}, profiles=ps)
+        _assert_same_hits(a, b)
+        total += len(b)
+    assert total > 0
+
+
+def test_search_viral_screen_shape(engine):
+    """Viral-screen shape (shrunk): many profiles of M 30-800 against short
+    targets with skewed residue frequencies, E-value cutoffs, filters on."""
+    w = small_config(4, 0.002)
+    seqs = [(w.target_ids[i], _decode(s)) for i, s in enumerate(w.targets)]
+    _cmp(engine, w.hmm_text(), seqs, filters=True)
+    _cmp(engine, w.hmm_text(), seqs[:60], filters=False)
+
+
 def test_missing_cutoff_raises_like_reference(engine):
     ps = engine.load_text(tiny_text())
     with pytest.raises(sxhmm.HmmError, match="TC bit thresholds unavailable on model tiny"):

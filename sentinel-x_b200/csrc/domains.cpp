@@ -925,6 +925,7 @@ bool is_multidomain(const std::vector<float>& btot, const std::vector<float>& et
 }  // namespace
 
 float forward_score_from_rows(const ProfileHost& p, int64_t l, const float* fwd_rows) {
+  if (l <= 0) return kNegInf;  // no row was computed; the reference's xc stays 0
   LogRows sp;
   double lnscale;
   forward_log_rows(p, l, fwd_rows, sp, lnscale);
@@ -934,6 +935,7 @@ float forward_score_from_rows(const ProfileHost& p, int64_t l, const float* fwd_
 }
 
 float backward_score_from_rows(int64_t l, const float* bwd_rows) {
+  if (l <= 0) return kNegInf;
   LogRows sp;
   return backward_log_rows(l, bwd_rows, sp);
 }

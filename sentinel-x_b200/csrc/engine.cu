@@ -40,7 +40,7 @@
 #include "internal.hpp"
 #include "kernels.cuh"
 #include "adjoint.cuh"
-#include "plain.cuh"
+#include "long.cuh"
 #include "envelope.cuh"
 
 using namespace sx;
@@ -128,7 +128,9 @@ constexpr MsvShape kMsvShapes[] = {
     {2, 36}, {2, 44}, {2, 52}, {2, 60}, {4, 36}, {4, 44}, {4, 52}, {4, 60},
     {8, 36}, {8, 44}, {8, 52}, {8, 60}};
 constexpr int kNumMsvShapes = sizeof(kMsvShapes) / sizeof(kMsvShapes[0]);
-constexpr int kMaxM = 2048;
+constexpr int kMaxM = 2048;  // columns of the warp-chunked and lane-group kernels
+// Longer profiles (marker models of long proteins) run through the long kernels.
+inline bool is_long(int m) { return m > kMaxM; }
 // Viterbi lane-group shapes (G lanes per pair, C columns per lane).
 // Viterbi lane-group shapes: G lanes per pair, C columns per lane, rt = the
 // transition rows held in registers for the whole pair (C <= 16).
@@ -514,6 +516,9 @@ struct sx_engine {
   DevBuf<sxk::TraceRec> trc_recs;  // stochastic-trace passes of multi-domain regions
   DevBuf<int32_t> trc_pool, trc_count, trc_status;
   DevBuf<float> trc_cols;
+  DevBuf<sxk::LongPair> long_pairs;  // pairs of profiles longer than kMaxM
+  DevBuf<float> long_scratch, long_out, long_rows_f, long_rows_b;
+  DevBuf<int64_t> long_row_off;
   DevBuf<Thresholds> thr;
   DevBuf<float> rows_f, rows_b;
   DevBuf<int64_t> row_off;
@@ -580,6 +585,122 @@ void join_aux(Streams& X) {
 }
 
 // ---- profile packing --------------------------------------------------------
+// The images of a profile the warp-chunked and lane-group kernels read.
+void pack_images(const ProfileHost& h, const DevProfile& d, float4* msv, float4* vit, float* vfb) {
+  const int m = h.m;
+  // MSV image: residue row x, float4 chunk c4 of lane j at (x*NC4 + c4)*G + j;
+  // lane j's column c is k = j*C + c + 1.
+  {
+    const int G = d.msv_g, C = d.msv_c, NC4 = C / 4;
+    float4* base = msv + d.msv_off;
+    for (int x = 0; x < 25; x++)
+      for (int j = 0; j < G; j++)
+        for (int c4 = 0; c4 < NC4; c4++) {
+          float v[4];
+          for (int e = 0; e < 4; e++) {
+            const int k = j * C + c4 * 4 + e + 1;
+            v[e] = k <= m ? h.msc_row(x)[k] : kNegInf;
+          }
+          base[((size_t)x * NC4 + c4) * G + j] = make_float4(v[0], v[1], v[2], v[3]);
+        }
+  }
+  // Viterbi image: rows 0..24 log-odds, 25..32 transitions (mm im dm at k-1, bm mi ii at k,
+  // md dd at k-1), lane-major float4 chunks as for MSV
+  {
+    const int G = kVitShapes[d.vshape].g, C = kVitShapes[d.vshape].c, NC4 = C / 4;
+    float4* base = vit + d.vit_off;
+    auto row = [&](int r, const std::function<float(int)>& f, float pad) {
+      for (int j = 0; j < G; j++)
+        for (int c4 = 0; c4 < NC4; c4++) {
+          float v[4];
+          for (int e = 0; e < 4; e++) {
+            const int k = j * C + c4 * 4 + e + 1;
+            v[e] = k <= m ? f(k) : pad;
+          }
+          base[((size_t)r * NC4 + c4) * G + j] = make_float4(v[0], v[1], v[2], v[3]);
+        }
+    };
+    for (int x = 0; x < 25; x++) row(x, [&](int k) { return h.msc_row(x)[k]; }, kNegInf);
+    const auto& t = h.t;
+    row(25, [&](int k) { return t[TMM][k - 1]; }, kNegInf);
+    row(26, [&](int k) { return t[TIM][k - 1]; }, kNegInf);
+    row(27, [&](int k) { return t[TDM][k - 1]; }, kNegInf);
+    row(28, [&](int k) { return t[TBM][k]; }, kNegInf);
+    // no insert state at node M: -inf from k = M on keeps I_M.. at -inf
+    row(29, [&](int k) { return k < m ? t[TMI][k] : kNegInf; }, kNegInf);
+    row(30, [&](int k) { return k < m ? t[TII][k] : kNegInf; }, kNegInf);
+    row(31, [&](int k) { return t[TMD][k - 1]; }, kNegInf);
+    row(32, [&](int k) { return t[TDD][k - 1]; }, kNegInf);
+  }
+  // warp-chunked image: row r, lane l, column c (k = l*vc + c + 1) at (r*vc + c)*32 + l
+  {
+    const int vc = d.vc;
+    float* base = vfb + d.vfb_off;
+    auto put = [&](int r, const std::function<float(int)>& f, float pad) {
+      for (int l = 0; l < 32; l++)
+        for (int c = 0; c < vc; c++) {
+          const int k = l * vc + c + 1;
+          base[((size_t)r * vc + c) * 32 + l] = k <= m ? f(k) : pad;
+        }
+    };
+    for (int x = 0; x < 25; x++) {
+      put(sxk::kRowMsc + x, [&](int k) { return h.msc_row(x)[k]; }, kNegInf);
+      put(sxk::kRowMo + x, [&](int k) { return h.mo_row(x)[k]; }, 0.0f);
+    }
+    const auto& t = h.t;
+    const auto& p = h.p;
+    auto shl = [&](const std::vector<float>& v) { return [&v](int k) { return v[k - 1]; }; };
+    auto at = [&](const std::vector<float>& v) { return [&v](int k) { return v[k]; }; };
+    put(sxk::kRowVit + 0, shl(t[TMM]), kNegInf);
+    put(sxk::kRowVit + 1, shl(t[TIM]), kNegInf);
+    put(sxk::kRowVit + 2, shl(t[TDM]), kNegInf);
+    put(sxk::kRowVit + 3, at(t[TBM]), kNegInf);
+    put(sxk::kRowVit + 4, at(t[TMI]), kNegInf);
+    put(sxk::kRowVit + 5, at(t[TII]), kNegInf);
+    put(sxk::kRowVit + 6, shl(t[TMD]), kNegInf);
+    put(sxk::kRowVit + 7, shl(t[TDD]), kNegInf);
+    put(sxk::kRowFwd + 0, at(p[TBM]), 0.0f);
+    put(sxk::kRowFwd + 1, shl(p[TMM]), 0.0f);
+    put(sxk::kRowFwd + 2, shl(p[TIM]), 0.0f);
+    put(sxk::kRowFwd + 3, shl(p[TDM]), 0.0f);
+    put(sxk::kRowFwd + 4, at(p[TMI]), 0.0f);
+    put(sxk::kRowFwd + 5, at(p[TII]), 0.0f);
+    put(sxk::kRowFwd + 6, shl(p[TMD]), 0.0f);
+    put(sxk::kRowFwd + 7, shl(p[TDD]), 0.0f);
+    put(sxk::kRowBwd + 0, at(p[TMM]), 0.0f);
+    put(sxk::kRowBwd + 1, at(p[TMI]), 0.0f);
+    put(sxk::kRowBwd + 2, at(p[TMD]), 0.0f);
+    put(sxk::kRowBwd + 3, at(p[TIM]), 0.0f);
+    put(sxk::kRowBwd + 4, at(p[TII]), 0.0f);
+    put(sxk::kRowBwd + 5, at(p[TDM]), 0.0f);
+    put(sxk::kRowBwd + 6, at(p[TDD]), 0.0f);
+    put(sxk::kRowBwd + 7, at(p[TBM]), 0.0f);
+  }
+}
+
+// Composition-bias filter table (src/hmmer/pipeline.rs:110-131): 54 doubles.
+void pack_bias(const ProfileHost& h, double* b) {
+  const int m = h.m;
+  for (int x = 0; x < 25; x++) b[x] = b[25 + x] = 1.0;
+  for (int x = 0; x < NRES; x++) b[25 + x] = (double)h.compo[x] / (double)kBackground[x];
+  for (int code = 20; code <= 23; code++) {
+    const Degenerate& dg = degenerate(code);
+    double e0 = 0, e1 = 0, z = 0;
+    for (int q = 0; q < dg.n; q++) {
+      e0 += (double)kBackground[dg.members[q]];
+      e1 += (double)h.compo[dg.members[q]];
+      z += (double)kBackground[dg.members[q]];
+    }
+    b[code] = e0 / z;
+    b[25 + code] = e1 / z;
+  }
+  const double l0 = 400.0, l1 = (double)m / 8.0;
+  b[50] = l0 / (l0 + 1.0);
+  b[51] = 1.0 / (l0 + 1.0);
+  b[52] = 1.0 / (l1 + 1.0);
+  b[53] = l1 / (l1 + 1.0);
+}
+
 void pack_profiles(sx_profiles* P) {
   const size_t np = P->h.size();
   P->dp.resize(np);
@@ -590,11 +711,18 @@ void pack_profiles(sx_profiles* P) {
     DevProfile& d = P->dp[i];
     memset(&d, 0, sizeof d);
     d.m = h.m;
+    d.msv_tbm = h.msv_tbm;
+    if (is_long(h.m)) {  // no warp-chunked, MSV or Viterbi images: the long kernels read the plain image
+      P->msv_shape[i] = -1;
+      d.vbin = d.vshape = -1;
+      d.msv_off = msv_total;
+      d.vfb_off = vfb_total;
+      d.vit_off = vit_total;
+      continue;
+    }
     const int s = choose_msv_shape(h.m);
     const int vb = choose_vbin(h.m);
-    if (s < 0 || vb < 0)
-      throw CudaError{SX_EINVAL, "profile '" + h.name + "' has M=" + std::to_string(h.m) +
-                                     " nodes; this build supports M <= " + std::to_string(kMaxM)};
+    if (s < 0 || vb < 0) throw CudaError{SX_EINVAL, "profile '" + h.name + "': no kernel shape for M=" + std::to_string(h.m)};
     P->msv_shape[i] = s;
     d.msv_g = kMsvShapes[s].g;
     d.msv_c = kMsvShapes[s].c;
@@ -604,7 +732,6 @@ void pack_profiles(sx_profiles* P) {
     msv_total += 25LL * (d.msv_c / 4) * d.msv_g;
     d.vfb_off = vfb_total;
     vfb_total += (int64_t)sxk::kImgRows * 32 * d.vc;
-    d.msv_tbm = h.msv_tbm;
     d.vshape = choose_vit_shape(h.m);
     if (d.vshape < 0) throw CudaError{SX_EINVAL, "profile '" + h.name + "' too long for the Viterbi shapes"};
     d.vit_off = vit_total;
@@ -615,128 +742,19 @@ void pack_profiles(sx_profiles* P) {
   std::vector<float> vfb((size_t)vfb_total);
   std::vector<double> bias(np * 54);
   for (size_t i = 0; i < np; i++) {
-    const ProfileHost& h = P->h[i];
-    const DevProfile& d = P->dp[i];
-    const int m = h.m;
-    // MSV image: residue row x, float4 chunk c4 of lane j at (x*NC4 + c4)*G + j;
-    // lane j's column c is k = j*C + c + 1.
-    {
-      const int G = d.msv_g, C = d.msv_c, NC4 = C / 4;
-      float4* base = msv.data() + d.msv_off;
-      for (int x = 0; x < 25; x++)
-        for (int j = 0; j < G; j++)
-          for (int c4 = 0; c4 < NC4; c4++) {
-            float v[4];
-            for (int e = 0; e < 4; e++) {
-              const int k = j * C + c4 * 4 + e + 1;
-              v[e] = k <= m ? h.msc_row(x)[k] : kNegInf;
-            }
-            base[((size_t)x * NC4 + c4) * G + j] = make_float4(v[0], v[1], v[2], v[3]);
-          }
-    }
-    // Viterbi image: rows 0..24 log-odds, 25..32 transitions (mm im dm at k-1, bm mi ii at k,
-    // md dd at k-1), lane-major float4 chunks as for MSV
-    {
-      const int G = kVitShapes[d.vshape].g, C = kVitShapes[d.vshape].c, NC4 = C / 4;
-      float4* base = vit.data() + d.vit_off;
-      auto row = [&](int r, const std::function<float(int)>& f, float pad) {
-        for (int j = 0; j < G; j++)
-          for (int c4 = 0; c4 < NC4; c4++) {
-            float v[4];
-            for (int e = 0; e < 4; e++) {
-              const int k = j * C + c4 * 4 + e + 1;
-              v[e] = k <= m ? f(k) : pad;
-            }
-            base[((size_t)r * NC4 + c4) * G + j] = make_float4(v[0], v[1], v[2], v[3]);
-          }
-      };
-      for (int x = 0; x < 25; x++) row(x, [&](int k) { return h.msc_row(x)[k]; }, kNegInf);
-      const auto& t = h.t;
-      row(25, [&](int k) { return t[TMM][k - 1]; }, kNegInf);
-      row(26, [&](int k) { return t[TIM][k - 1]; }, kNegInf);
-      row(27, [&](int k) { return t[TDM][k - 1]; }, kNegInf);
-      row(28, [&](int k) { return t[TBM][k]; }, kNegInf);
-      // no insert state at node M: -inf from k = M on keeps I_M.. at -inf
-      row(29, [&](int k) { return k < m ? t[TMI][k] : kNegInf; }, kNegInf);
-      row(30, [&](int k) { return k < m ? t[TII][k] : kNegInf; }, kNegInf);
-      row(31, [&](int k) { return t[TMD][k - 1]; }, kNegInf);
-      row(32, [&](int k) { return t[TDD][k - 1]; }, kNegInf);
-    }
-    // warp-chunked image: row r, lane l, column c (k = l*vc + c + 1) at (r*vc + c)*32 + l
-    {
-      const int vc = d.vc;
-      float* base = vfb.data() + d.vfb_off;
-      auto put = [&](int r, const std::function<float(int)>& f, float pad) {
-        for (int l = 0; l < 32; l++)
-          for (int c = 0; c < vc; c++) {
-            const int k = l * vc + c + 1;
-            base[((size_t)r * vc + c) * 32 + l] = k <= m ? f(k) : pad;
-          }
-      };
-      for (int x = 0; x < 25; x++) {
-        put(sxk::kRowMsc + x, [&](int k) { return h.msc_row(x)[k]; }, kNegInf);
-        put(sxk::kRowMo + x, [&](int k) { return h.mo_row(x)[k]; }, 0.0f);
-      }
-      const auto& t = h.t;
-      const auto& p = h.p;
-      auto shl = [&](const std::vector<float>& v) { return [&v](int k) { return v[k - 1]; }; };
-      auto at = [&](const std::vector<float>& v) { return [&v](int k) { return v[k]; }; };
-      put(sxk::kRowVit + 0, shl(t[TMM]), kNegInf);
-      put(sxk::kRowVit + 1, shl(t[TIM]), kNegInf);
-      put(sxk::kRowVit + 2, shl(t[TDM]), kNegInf);
-      put(sxk::kRowVit + 3, at(t[TBM]), kNegInf);
-      put(sxk::kRowVit + 4, at(t[TMI]), kNegInf);
-      put(sxk::kRowVit + 5, at(t[TII]), kNegInf);
-      put(sxk::kRowVit + 6, shl(t[TMD]), kNegInf);
-      put(sxk::kRowVit + 7, shl(t[TDD]), kNegInf);
-      put(sxk::kRowFwd + 0, at(p[TBM]), 0.0f);
-      put(sxk::kRowFwd + 1, shl(p[TMM]), 0.0f);
-      put(sxk::kRowFwd + 2, shl(p[TIM]), 0.0f);
-      put(sxk::kRowFwd + 3, shl(p[TDM]), 0.0f);
-      put(sxk::kRowFwd + 4, at(p[TMI]), 0.0f);
-      put(sxk::kRowFwd + 5, at(p[TII]), 0.0f);
-      put(sxk::kRowFwd + 6, shl(p[TMD]), 0.0f);
-      put(sxk::kRowFwd + 7, shl(p[TDD]), 0.0f);
-      put(sxk::kRowBwd + 0, at(p[TMM]), 0.0f);
-      put(sxk::kRowBwd + 1, at(p[TMI]), 0.0f);
-      put(sxk::kRowBwd + 2, at(p[TMD]), 0.0f);
-      put(sxk::kRowBwd + 3, at(p[TIM]), 0.0f);
-      put(sxk::kRowBwd + 4, at(p[TII]), 0.0f);
-      put(sxk::kRowBwd + 5, at(p[TDM]), 0.0f);
-      put(sxk::kRowBwd + 6, at(p[TDD]), 0.0f);
-      put(sxk::kRowBwd + 7, at(p[TBM]), 0.0f);
-    }
-    // composition-bias filter table (src/hmmer/pipeline.rs:110-131)
-    {
-      double* b = bias.data() + i * 54;
-      for (int x = 0; x < 25; x++) b[x] = b[25 + x] = 1.0;
-      for (int x = 0; x < NRES; x++) b[25 + x] = (double)h.compo[x] / (double)kBackground[x];
-      for (int code = 20; code <= 23; code++) {
-        const Degenerate& dg = degenerate(code);
-        double e0 = 0, e1 = 0, z = 0;
-        for (int q = 0; q < dg.n; q++) {
-          e0 += (double)kBackground[dg.members[q]];
-          e1 += (double)h.compo[dg.members[q]];
-          z += (double)kBackground[dg.members[q]];
-        }
-        b[code] = e0 / z;
-        b[25 + code] = e1 / z;
-      }
-      const double l0 = 400.0, l1 = (double)m / 8.0;
-      b[50] = l0 / (l0 + 1.0);
-      b[51] = 1.0 / (l0 + 1.0);
-      b[52] = 1.0 / (l1 + 1.0);
-      b[53] = l1 / (l1 + 1.0);
-    }
+    if (P->dp[i].vbin >= 0) pack_images(P->h[i], P->dp[i], msv.data(), vit.data(), vfb.data());
+    pack_bias(P->h[i], bias.data() + i * 54);
   }
-  // plain layout: 25 msc rows then mm mi md im ii dm dd bm, each M+1 long
+  // plain layout: 25 msc rows then mm mi md im ii dm dd bm, each M+1 long;
+  // long profiles add the 25 odds rows and the 8 probability rows (same order),
+  // the image of the long kernels
   std::vector<sxk::PlainProfile> pprof(np);
   int64_t plain_total = 0;
   for (size_t i = 0; i < np; i++) {
     pprof[i].off = plain_total;
     pprof[i].m = P->h[i].m;
     pprof[i].pad = 0;
-    plain_total += 33LL * (P->h[i].m + 1);
+    plain_total += (is_long(P->h[i].m) ? (int64_t)sxk::kLongRows : 33LL) * (P->h[i].m + 1);
   }
   std::vector<float> plain((size_t)std::max<int64_t>(plain_total, 1));
   for (size_t i = 0; i < np; i++) {
@@ -746,6 +764,10 @@ void pack_profiles(sx_profiles* P) {
     memcpy(b, h.msc.data(), sizeof(float) * 25 * w);
     const int order[8] = {TMM, TMI, TMD, TIM, TII, TDM, TDD, TBM};
     for (int q = 0; q < 8; q++) memcpy(b + (25 + q) * w, h.t[order[q]].data(), sizeof(float) * w);
+    if (is_long(h.m)) {
+      memcpy(b + sxk::kLMo * w, h.mo.data(), sizeof(float) * 25 * w);
+      for (int q = 0; q < 8; q++) memcpy(b + (sxk::kLP + q) * w, h.p[order[q]].data(), sizeof(float) * w);
+    }
   }
   cudaStream_t s = P->eng->stream;
   P->d_pprof.upload(pprof.data(), np, s);
@@ -1146,8 +1168,9 @@ std::vector<std::vector<MsvTile>> make_all_pairs_tiles(const sx_engine* E, const
   std::iota(pord.begin(), pord.end(), p0);
   std::stable_sort(pord.begin(), pord.end(), [&](int a, int b) { return P->h[a].m > P->h[b].m; });
   for (int pi : pord)
-    for (int s = 0; s < nslices; s++)
-      if (cut[s + 1] > cut[s]) by_shape[P->msv_shape[pi]].push_back({pi, cut[s], cut[s + 1], 0});
+    if (P->msv_shape[pi] >= 0)
+      for (int s = 0; s < nslices; s++)
+        if (cut[s + 1] > cut[s]) by_shape[P->msv_shape[pi]].push_back({pi, cut[s], cut[s + 1], 0});
   return by_shape;
 }
 
@@ -1559,6 +1582,88 @@ RegionPassStats region_passes(sx_engine* E, const sx_profiles* P, const sx_targe
   return st;
 }
 
+// ---- profiles longer than kMaxM ----------------------------------------------
+// One CTA per pair; each CTA keeps kLongArrays rows of M+1 floats in scratch.
+constexpr int kLongCtasPerSm = 8;
+
+int long_grid(const sx_engine* E, size_t n) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)n, (int64_t)E->num_sms * kLongCtasPerSm));
+}
+int64_t long_stride(const sx_profiles* P, const std::vector<sxk::LongPair>& v, size_t a, size_t b) {
+  int m = 0;
+  for (size_t i = a; i < b; i++) m = std::max(m, P->h[v[i].p].m);
+  return (int64_t)sxk::kLongArrays * (m + 1);
+}
+
+// MSV (viterbi = false) or Viterbi scores of long-profile pairs.
+void long_scores(sx_engine* E, const sx_profiles* P, const sx_targets* T, const std::vector<sxk::LongPair>& v,
+                 bool viterbi, std::vector<float>& out) {
+  out.assign(v.size(), kNegInf);
+  if (v.empty()) return;
+  cudaStream_t s = E->stream;
+  const int grid = long_grid(E, v.size());
+  const int64_t stride = long_stride(P, v, 0, v.size());
+  E->long_pairs.upload(v.data(), v.size(), s);
+  E->long_scratch.alloc((size_t)grid * (size_t)stride);
+  E->long_out.alloc(v.size());
+  if (viterbi)
+    sxk::long_viterbi_kernel<<<grid, sxk::kPlainThreads, 0, s>>>(E->long_pairs.p, (int)v.size(), P->d_pprof.p,
+                                                                P->d_plain.p, T->d_res.p, T->d_off.p, T->d_len.p,
+                                                                T->d_xsc.p, E->long_scratch.p, stride, E->long_out.p);
+  else
+    sxk::long_msv_kernel<<<grid, sxk::kPlainThreads, 0, s>>>(E->long_pairs.p, (int)v.size(), P->d_pprof.p,
+                                                            P->d_plain.p, P->d_prof.p, T->d_res.p, T->d_off.p,
+                                                            T->d_len.p, T->d_tpar.p, E->long_scratch.p, stride,
+                                                            E->long_out.p);
+  CK(cudaGetLastError());
+  E->stats.kernel_launches++;
+  CK(cudaMemcpyAsync(out.data(), E->long_out.p, sizeof(float) * v.size(), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+}
+
+// Raw Forward/Backward special rows of long-profile pairs, in chunks bounded
+// by the scratch budget; consume(first, n, fwd, bwd, off) per chunk, pair
+// first + q having its rows at fwd + off[q] and bwd + off[q].
+template <typename F>
+void long_rows(sx_engine* E, const sx_profiles* P, const sx_targets* T, const std::vector<sxk::LongPair>& v,
+               F&& consume) {
+  cudaStream_t s = E->stream;
+  const int64_t budget = std::max<int64_t>(scratch_budget(E, E->batch_bytes / 2) / (int64_t)sizeof(float), 1 << 20);
+  size_t i0 = 0;
+  while (i0 < v.size()) {
+    size_t i1 = i0;
+    int64_t used = 0;
+    std::vector<int64_t> off;
+    while (i1 < v.size()) {
+      const int64_t need = 6 * ((int64_t)T->len[v[i1].t] + 1);
+      if (i1 > i0 && used + need > budget) break;
+      off.push_back(used);
+      used += need;
+      i1++;
+    }
+    const size_t n = i1 - i0;
+    const int grid = long_grid(E, n);
+    const int64_t stride = long_stride(P, v, i0, i1);
+    E->long_pairs.upload(v.data() + i0, n, s);
+    E->long_row_off.upload(off.data(), n, s);
+    E->long_scratch.alloc((size_t)grid * (size_t)stride);
+    E->long_rows_f.alloc((size_t)used);
+    E->long_rows_b.alloc((size_t)used);
+    sxk::long_rows_kernel<<<grid, sxk::kPlainThreads, 0, s>>>(E->long_pairs.p, (int)n, P->d_pprof.p, P->d_plain.p,
+                                                             T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p,
+                                                             E->long_scratch.p, stride, E->long_rows_f.p,
+                                                             E->long_rows_b.p, E->long_row_off.p);
+    CK(cudaGetLastError());
+    E->stats.kernel_launches++;
+    std::vector<float> f((size_t)used), b((size_t)used);
+    CK(cudaMemcpyAsync(f.data(), E->long_rows_f.p, sizeof(float) * (size_t)used, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(b.data(), E->long_rows_b.p, sizeof(float) * (size_t)used, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    consume(i0, n, f.data(), b.data(), off);
+    i0 = i1;
+  }
+}
+
 // Contiguous ranges of profile indices with about equal filtered DP cells.
 // Each range runs through the device cascade as one block; the host domain
 // definition of a block overlaps the device work of the blocks after it.
@@ -1615,7 +1720,7 @@ void cascade_launch(sx_engine* E, Slot& S, const sx_profiles* P, const sx_target
     R.pairs_in_vs.assign(kMaxBins, 0.0);
     R.cells_total = 0;
     for (int pi = R.p0; pi < R.p1; pi++)
-      if (th[pi].exact) {
+      if (th[pi].exact && P->dp[pi].vbin >= 0) {
         R.pairs_in_bin[P->dp[pi].vbin] += (double)nt;
         R.pairs_in_vs[P->dp[pi].vshape] += (double)nt;
         R.cells_total += (double)P->h[pi].m * T->residues;
@@ -1767,6 +1872,15 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
   const size_t np = P->h.size(), nt = T->len.size();
   cudaStream_t s = E->stream;
   std::vector<Thresholds> th = make_thresholds(P->h, o);
+  // profiles longer than kMaxM take the long pass instead of the cascade
+  std::vector<int> longs;
+  std::vector<char> long_exact(np, 0);
+  for (size_t pi = 0; pi < np; pi++)
+    if (is_long(P->h[pi].m)) {
+      longs.push_back((int)pi);
+      long_exact[pi] = (char)th[pi].exact;
+      th[pi].exact = 0;
+    }
   E->thr.upload(th.data(), th.size(), s);
   for (Slot& S : E->sl) {
     S.overflow.alloc(1);
@@ -1921,7 +2035,7 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
 
   std::vector<int> unfiltered;
   for (size_t pi = 0; pi < np; pi++)
-    if (!th[pi].exact) unfiltered.push_back((int)pi);
+    if (!th[pi].exact && !is_long(P->h[pi].m)) unfiltered.push_back((int)pi);
   int64_t nfinal = 0;
   // software pipeline over two slots: block b+1's MSV is queued on the device
   // before block b's later stages are driven, so it fills the GPU around
@@ -1986,6 +2100,70 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
       pb.B->res[i].hit = pb.db->finish(q, pb.F, pb.D, pb.B->res[i].h);
     });
     E->stats.ms[5] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_env).count();
+  }
+  // profiles longer than kMaxM: MSV on the device, the exact host checks of the
+  // F1 / bias / F2 filters on its scores (those cascade_finish re-runs), the
+  // Viterbi scores of the survivors, then the rows of the final pairs, F3 and
+  // domain definition on the host pool
+  if (!longs.empty() && nt > 0) {
+    outs.push_back(std::make_unique<BlockOut>());
+    BlockOut* B = outs.back().get();
+    std::vector<sxk::LongPair> filt;
+    for (int pi : longs)
+      for (size_t t = 0; t < nt; t++) {
+        if (long_exact[pi]) filt.push_back({pi, (int32_t)t});
+        else B->finals.push_back({pi, (int32_t)t, 0.f, 0.f, 0.f, -1});
+      }
+    std::vector<float> usc, vsc, fsc(filt.size(), 0.f);
+    long_scores(E, P, T, filt, false, usc);
+    std::vector<char> pass1(filt.size(), 0);
+    parallel_for(filt.size(), E->host_threads, [&](size_t i) {
+      const ProfileHost& h = P->h[filt[i].p];
+      const int64_t l = T->len[filt[i].t];
+      const float nullsc = null1_score(l);
+      if (gumbel_survival((double)((usc[i] - nullsc) / kLn2f), h.msv[0], h.msv[1]) > o.f1) return;
+      fsc[i] = composition_bias_score(h, T->dsq.data() + T->off[filt[i].t], l);
+      if (gumbel_survival((double)((usc[i] - fsc[i]) / kLn2f), h.msv[0], h.msv[1]) > o.f1) return;
+      pass1[i] = 1;
+    });
+    std::vector<sxk::LongPair> surv;
+    std::vector<size_t> from;
+    for (size_t i = 0; i < filt.size(); i++)
+      if (pass1[i]) {
+        surv.push_back(filt[i]);
+        from.push_back(i);
+      }
+    long_scores(E, P, T, surv, true, vsc);
+    for (size_t q = 0; q < surv.size(); q++) {
+      const size_t i = from[q];
+      const ProfileHost& h = P->h[surv[q].p];
+      if (gumbel_survival((double)((vsc[q] - fsc[i]) / kLn2f), h.vit[0], h.vit[1]) > o.f2) continue;
+      B->finals.push_back({surv[q].p, surv[q].t, usc[i], fsc[i], vsc[q], -1});
+    }
+    for (const sxk::LongPair& q : filt) {
+      E->stats.pairs_in[0]++;
+      E->stats.cells[0] += (double)P->h[q.p].m * (double)T->len[q.t];
+    }
+    B->res.resize(B->finals.size());
+    std::vector<sxk::LongPair> fin(B->finals.size());
+    for (size_t i = 0; i < fin.size(); i++) fin[i] = {B->finals[i].p, B->finals[i].t};
+    nfinal += (int64_t)fin.size();
+    long_rows(E, P, T, fin, [&](size_t first, size_t n, const float* f, const float* b, const std::vector<int64_t>& off) {
+      parallel_for(n, E->host_threads, [&](size_t q) {
+        const size_t i = first + q;
+        const FinalPair& fp = B->finals[i];
+        const ProfileHost& h = P->h[fp.p];
+        const int64_t l = T->len[fp.t];
+        const float* fr = f + off[q];
+        const float* br = b + off[q];
+        const float fwdsc = forward_score_from_rows(h, l, fr);
+        if (long_exact[fp.p] &&
+            std::exp(exp_tail_logsurv((double)((fwdsc - fp.filtersc) / kLn2f), h.fwd[0], h.fwd[1])) > o.f3)
+          return;
+        n_domain++;
+        B->res[i].hit = define_domains(h, T->dsq.data() + T->off[fp.t], l, RawRows{fr, br}, fwdsc, o, B->res[i].h);
+      });
+    });
   }
   E->stats.kernel_launches += env_launches.load();
   E->stats.pairs_out[5] = n_env.load();
@@ -2375,6 +2553,14 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
     e->overflow.alloc(1);
     CK(cudaMemsetAsync(e->overflow.p, 0, sizeof(unsigned), s));
     e->scores.alloc(npairs);
+    // pairs of profiles longer than kMaxM go through the long kernels
+    std::vector<size_t> lng;
+    std::vector<sxk::LongPair> lpairs;
+    for (size_t i = 0; i < npairs; i++)
+      if (is_long(p->h[pair_profile[i]].m)) {
+        lng.push_back(i);
+        lpairs.push_back({pair_profile[i], pair_target[i]});
+      }
     if (msv) {
       // list sorted by (profile, length desc); tiles per profile over that list
       std::vector<int32_t> idx(npairs);
@@ -2394,8 +2580,9 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
         size_t r = q;
         const int pp = pair_profile[idx[q]];
         while (r < npairs && pair_profile[idx[r]] == pp) r++;
-        for (size_t a = q; a < r; a += 4096)
-          tiles[p->msv_shape[pp]].push_back({pp, (int32_t)a, (int32_t)std::min(r, a + 4096), 0});
+        if (p->msv_shape[pp] >= 0)
+          for (size_t a = q; a < r; a += 4096)
+            tiles[p->msv_shape[pp]].push_back({pp, (int32_t)a, (int32_t)std::min(r, a + 4096), 0});
         q = r;
       }
       e->plist.upload(lst.data(), npairs, s);
@@ -2403,6 +2590,11 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
       launch_msv(e, e->sl[0], e->sl[0].hi, p, t, tiles, e->plist.p, e->scores.p, e->slots.p, nullptr, nullptr, nullptr);
       CK(cudaMemcpyAsync(msv, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
+      if (!lng.empty()) {
+        std::vector<float> v;
+        long_scores(e, p, t, lpairs, false, v);
+        for (size_t q = 0; q < lng.size(); q++) msv[lng[q]] = v[q];
+      }
     }
     if (bias || viterbi) {
       // pair lists per vbin, every pair carries its slot
@@ -2410,7 +2602,11 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
       std::vector<BinRegion> reg(kMaxBins);
       std::vector<unsigned> cnt(kMaxBins, 0);
       std::vector<std::vector<int32_t>> byb(kMaxBins);
-      for (size_t i = 0; i < npairs; i++) byb[p->dp[pair_profile[i]].vshape].push_back((int32_t)i);
+      // long-profile pairs sit in an extra bin that only the bias pass reads
+      for (size_t i = 0; i < npairs; i++) {
+        const int vs = p->dp[pair_profile[i]].vshape;
+        byb[vs >= 0 ? vs : kNumVitShapes].push_back((int32_t)i);
+      }
       for (int b = 0; b < kMaxBins; b++) {
         reg[b].off = (int64_t)recs.size();
         reg[b].cap = (uint32_t)byb[b].size();
@@ -2426,7 +2622,7 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
       if (bias) {
         unsigned mx = *std::max_element(cnt.begin(), cnt.end());
         dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>((mx + 255) / 256, (int64_t)e->num_sms * 8)),
-                  kNumVitShapes);
+                  kNumVitShapes + 1);
         sxk::bias_kernel<<<grid, 256, 0, s>>>(e->lists[0].p, e->counts.p, e->bins[0].p, nullptr, nullptr, nullptr,
                                               e->overflow.p, p->d_bias.p, e->thr.p, t->d_res.p, t->d_off.p, t->d_len.p,
                                               0.f, e->scores.p, p->d_prof.p);
@@ -2447,14 +2643,17 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(viterbi, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
+        if (!lng.empty()) {
+          std::vector<float> v;
+          long_scores(e, p, t, lpairs, true, v);
+          for (size_t q = 0; q < lng.size(); q++) viterbi[lng[q]] = v[q];
+        }
       }
     }
     if (forward || backward) {
-      std::vector<FinalPair> fp(npairs);
-      for (size_t i = 0; i < npairs; i++) fp[i] = {pair_profile[i], pair_target[i], 0.f, 0.f, 0.f, (int32_t)i};
-      rows_pass_sync(e, p, t, fp, [&](size_t i, const float* fr, const float* br) {
-        const ProfileHost& h = p->h[fp[i].p];
-        const int64_t l = t->len[fp[i].t];
+      auto put = [&](size_t i, const float* fr, const float* br) {
+        const ProfileHost& h = p->h[pair_profile[i]];
+        const int64_t l = t->len[pair_target[i]];
         if (l == 0 || h.m == 0) {
           if (forward) forward[i] = kNegInf;
           if (backward) backward[i] = kNegInf;
@@ -2462,6 +2661,13 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
         }
         if (forward) forward[i] = forward_score_from_rows(h, l, fr);
         if (backward) backward[i] = backward_score_from_rows(l, br);
+      };
+      std::vector<FinalPair> fp;
+      for (size_t i = 0; i < npairs; i++)
+        if (!is_long(p->h[pair_profile[i]].m)) fp.push_back({pair_profile[i], pair_target[i], 0.f, 0.f, 0.f, (int32_t)i});
+      rows_pass_sync(e, p, t, fp, [&](size_t q, const float* fr, const float* br) { put((size_t)fp[q].slot, fr, br); });
+      long_rows(e, p, t, lpairs, [&](size_t first, size_t n, const float* f, const float* b, const std::vector<int64_t>& off) {
+        for (size_t q = 0; q < n; q++) put(lng[first + q], f + off[q], b + off[q]);
       });
     }
   } catch (const CudaError& ce) {
@@ -2483,6 +2689,8 @@ int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, c
     if (p->h[pair_profile[i]].m != m)
       return fail(SX_EINVAL, "sx_posterior_grad: pair " + std::to_string(i) + " uses a profile of M=" +
                                  std::to_string(p->h[pair_profile[i]].m) + ", expected " + std::to_string(m));
+    if (is_long(m))
+      return fail(SX_EINVAL, "sx_posterior_grad: profiles of M > " + std::to_string(kMaxM) + " are not supported");
   }
   if (!npairs) return SX_OK;
   const int W = m + 1;
@@ -2643,6 +2851,8 @@ extern "C" int sx_score_viterbi_static(sx_engine* e, const sx_profiles* p, const
   for (size_t i = 0; i < npairs; i++) {
     if (pair_profile[i] < 0 || (size_t)pair_profile[i] >= np || pair_target[i] < 0 || (size_t)pair_target[i] >= nt)
       return fail(SX_EINVAL, "sx_score_viterbi_static: pair " + std::to_string(i) + " out of range");
+    if (p->dp[pair_profile[i]].vbin < 0)
+      return fail(SX_EINVAL, "sx_score_viterbi_static: profiles of M > " + std::to_string(kMaxM) + " are not supported");
     lay.n[p->dp[pair_profile[i]].vbin]++;
   }
   if (!npairs) return SX_OK;

@@ -14,8 +14,8 @@ import pytest
 
 from oracle import oracle as O
 import sxhmm
-from _workloads import (edge_targets, fixture_targets, fixture_text, small_config, small_profiles_text,
-                        tiny_text)
+from _workloads import (edge_targets, fixture_targets, fixture_text, long_workload, small_config,
+                        small_profiles_text, tiny_text)
 
 pytestmark = pytest.mark.gpu
 
@@ -191,6 +191,22 @@ def test_search_viral_screen_shape(engine):
     seqs = [(w.target_ids[i], _decode(s)) for i, s in enumerate(w.targets)]
     _cmp(engine, w.hmm_text(), seqs, filters=True)
     _cmp(engine, w.hmm_text(), seqs[:60], filters=False)
+
+
+def test_long_profiles(engine):
+    """Profiles longer than the warp-chunked kernels' 2048 columns (the long
+    kernels: one CTA per pair, rows in global scratch): stage scores
+    bit-identical to the oracle, and searches with filters on and off give the
+    oracle's hits, including an empty target."""
+    text, seqs = long_workload()
+    _stage_check(engine, text, [q for q in seqs if q[1]])
+    _, b = _cmp(engine, text, seqs, filters=True)
+    assert {(h[0], h[1]) for h in b} >= {(0, 5), (0, 6), (0, 7)}
+    _cmp(engine, text, seqs, cutoff="T", seq=-1e9, dom=-1e9, filters=False)
+    ps = engine.load_text(text)
+    ts = engine.targets([q[1] for q in seqs if q[1]])
+    with pytest.raises(sxhmm.HmmError, match="M > 2048"):
+        engine.posterior_grad(ps, ts, np.array([0], np.int32), np.array([5], np.int32), 2100)
 
 
 def test_missing_cutoff_raises_like_reference(engine):

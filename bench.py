@@ -18,6 +18,7 @@ Under torchrun (N > 1) each rank searches its own block of 1,000 profiles
 against the same targets (profile-block sharding, no data-path collective).
 """
 import argparse
+import gc
 import json
 import math
 import os
@@ -328,6 +329,12 @@ def main():
     # ---- device-resident steps ----
     for _ in range(args.warmup):
         eng.search(ps, ts, cfg)
+    # the interpreter's cyclic garbage collector stays off in the timed loops: a
+    # full collection over the workload's Python objects is a pause of this
+    # harness (tens of ms), not of the engine
+    gc.collect()
+    gc.freeze()
+    gc.disable()
     sampler = ClockSampler(local)
     sampler.start()
     times, launches, nhits = [], 0, 0
@@ -375,6 +382,7 @@ def main():
         e2e_parts.append([round((t_se - t_up) * 1e3, 1), round((t_sy - t_se) * 1e3, 1), round((t_cl - t_sy) * 1e3, 1)])
         e2e_stage.append({k: round(v, 1) for k, v in zip(STAGES, eng.stats()["ms"])})
         d2h = len(hits2) * 48 + len(doms2) * 56
+    gc.enable()
     # ---- MSV kernel alone: a single-block search, where MSV does not share the
     # GPU with later stages of another block, gives the kernel's own event time ----
     reng = sxhmm.Engine(device=local, pipeline_blocks=1)

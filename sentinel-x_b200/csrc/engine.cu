@@ -195,18 +195,19 @@ struct VitGTable<kNumVitShapes> {
 };
 template <int I>
 struct VbinTable {
-  static void fill(VitFn* v, FwdFn* f, BwdFn* b, AdjFFn* af, AdjBFn* ab) {
+  static void fill(VitFn* v, FwdFn* f, FwdFn* fs, BwdFn* b, AdjFFn* af, AdjBFn* ab) {
     v[I] = sxk::viterbi_kernel<kVcBins[I]>;
     f[I] = sxk::forward_kernel<kVcBins[I]>;
+    fs[I] = sxk::forward_kernel<kVcBins[I], true>;
     b[I] = sxk::backward_kernel<kVcBins[I]>;
     af[I] = sxk::adjoint_forward_kernel<kVcBins[I]>;
     ab[I] = sxk::adjoint_backward_kernel<kVcBins[I]>;
-    VbinTable<I + 1>::fill(v, f, b, af, ab);
+    VbinTable<I + 1>::fill(v, f, fs, b, af, ab);
   }
 };
 template <>
 struct VbinTable<kNumVbins> {
-  static void fill(VitFn*, FwdFn*, BwdFn*, AdjFFn*, AdjBFn*) {}
+  static void fill(VitFn*, FwdFn*, FwdFn*, BwdFn*, AdjFFn*, AdjBFn*) {}
 };
 
 typedef void (*EnvPassFn)(const sxk::EnvRec*, int, const DevProfile*, const float*, const uint8_t*, const int64_t*,
@@ -235,6 +236,7 @@ struct KernelTables {
   EnvPassFn regf[kNumVbins];
   VitFn vit[kNumVbins];
   FwdFn fwd[kNumVbins];
+  FwdFn fwd_scan[kNumVbins];  // the F3 pre-screen
   BwdFn bwd[kNumVbins];
   AdjFFn adjf[kNumVbins];
   AdjBFn adjb[kNumVbins];
@@ -242,7 +244,7 @@ struct KernelTables {
   KernelTables() {
     MsvTable<0>::fill(msv);
     VitGTable<0>::fill(vitg);
-    VbinTable<0>::fill(vit, fwd, bwd, adjf, adjb);
+    VbinTable<0>::fill(vit, fwd, fwd_scan, bwd, adjf, adjb);
     EnvTable<0>::fill(envf, envb, envp, regf);
   }
 };
@@ -1254,7 +1256,7 @@ void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets*
                                           S.overflow.p, P->d_prof.p, E->thr.p, P->d_vit.p, T->d_res.p, T->d_off.p,
                                           T->d_len.p, T->d_xsc.p, kSlackBits, nullptr, S.cursor.p);
       } else
-        K.fwd[b]<<<warp_ctas(E->num_sms, nin[b]), 32, 0, s>>>(S.lists[2].p, cin, S.bins[2].p, b, S.lists[3].p,
+        K.fwd_scan[b]<<<warp_ctas(E->num_sms, nin[b]), 32, 0, s>>>(S.lists[2].p, cin, S.bins[2].p, b, S.lists[3].p,
                                                                S.bins[3].p, cout,
                                         S.overflow.p, P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
                                         T->d_len.p, T->d_xsc.p, kSlackBits, nullptr, nullptr);

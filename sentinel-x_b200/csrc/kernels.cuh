@@ -488,8 +488,20 @@ __global__ void __launch_bounds__(256) viterbi_kernel(
 // matches.  Modes: rows != null writes the raw special rows (N B E J C, rescale
 // factor) per row i = 1..L; otherwise the pair passes when the device estimate
 // of the F3 statistic clears the threshold minus `slack`.
+//
+// SCAN (the F3 pre-screen only): the D chain is an affine recurrence
+// D[k] = a_k + D[k-1] p_k, so each lane forms its transfer (A, B) over its
+// columns, a Kogge-Stone scan of 5 shuffles composes them across lanes, each
+// lane re-runs its columns from the true carry-in, and the row sum is a
+// butterfly.  A row's dependent depth falls from ~2M to ~6 VC operations.  The
+// rounding differs from the reference's order, so the pass test adds a bound
+// on the difference: for sums and products of non-negative numbers the
+// relative errors of two evaluation orders add up along their longest paths,
+// at most 2^-24 per operation, i.e. |ln F_scan - ln F_ref| <=
+// (L+1)(2M + 6 VC + 64) 2^-24, taken twice.  The pre-screen therefore passes
+// every pair the exact F3 test (on the host, from exact rows) passes.
 // ===========================================================================
-template <int VC>
+template <int VC, bool SCAN = false>
 __global__ void __launch_bounds__(256) forward_kernel(
     const PairRec* __restrict__ in, const unsigned* __restrict__ in_counts, const BinRegion* __restrict__ in_bins,
     int bin, PairRec* __restrict__ out, const BinRegion* __restrict__ out_bins, unsigned* __restrict__ out_counts,
@@ -551,20 +563,51 @@ __global__ void __launch_bounds__(256) forward_kernel(
         a[c] = fmul(c ? mv[c - 1] : mcl, tr.get(img, kRowFwd, 6, c, lane));
         pdd[c] = tr.get(img, kRowFwd, 7, c, lane);
       }
-      // ordered D chain and row sum: dc[k] = a_k + dc[k-1]*p_dd[k-1]; xe += mv + dc
       float dcar = 0.f, xe = 0.f;
-      for (int sl = 0; sl < nl; sl++) {
-        if (lane == sl) {
+      if constexpr (SCAN) {
+        // lane transfer D_out = A + B D_in, then an inclusive scan over lanes
+        float A = 0.f, B = 1.f;
 #pragma unroll
-          for (int c = 0; c < VC; c++) {
-            const float d = fadd(a[c], fmul(dcar, pdd[c]));
-            dv[c] = d;
-            xe = fadd(xe, fadd(mv[c], d));
-            dcar = d;
+        for (int c = 0; c < VC; c++) {
+          A = fadd(a[c], fmul(A, pdd[c]));
+          B = fmul(B, pdd[c]);
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const float Au = __shfl_up_sync(kFull, A, o), Bu = __shfl_up_sync(kFull, B, o);
+          if (lane >= o) {
+            A = fadd(A, fmul(B, Au));
+            B = fmul(B, Bu);
           }
         }
-        dcar = __shfl_sync(kFull, dcar, sl);
-        xe = __shfl_sync(kFull, xe, sl);
+        const float din = __shfl_up_sync(kFull, A, 1);
+        dcar = lane ? din : 0.f;
+        float xl = 0.f;
+#pragma unroll
+        for (int c = 0; c < VC; c++) {
+          const float d = fadd(a[c], fmul(dcar, pdd[c]));
+          dv[c] = d;
+          xl = fadd(xl, fadd(mv[c], d));
+          dcar = d;
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) xl = fadd(xl, __shfl_xor_sync(kFull, xl, o));
+        xe = xl;
+      } else {
+        // ordered D chain and row sum: dc[k] = a_k + dc[k-1]*p_dd[k-1]; xe += mv + dc
+        for (int sl = 0; sl < nl; sl++) {
+          if (lane == sl) {
+#pragma unroll
+            for (int c = 0; c < VC; c++) {
+              const float d = fadd(a[c], fmul(dcar, pdd[c]));
+              dv[c] = d;
+              xe = fadd(xe, fadd(mv[c], d));
+              dcar = d;
+            }
+          }
+          dcar = __shfl_sync(kFull, dcar, sl);
+          xe = __shfl_sync(kFull, xe, sl);
+        }
       }
       if (lane >= nl) {
 #pragma unroll
@@ -608,7 +651,8 @@ __global__ void __launch_bounds__(256) forward_kernel(
       const float v = fmul(xc, pmove);
       const float fsc = (L > 0 && M > 0) ? (float)((double)(v > 0.f ? logf(v) : SX_NEG_INF) + lnscale) : SX_NEG_INF;
       r.fwd = fsc;
-      if (!rows && bits_stat(fsc, r.filtersc) >= thr[r.p].s3 - slack) push_pair(r, bin, out, out_bins, out_counts, overflow);
+      const float sl = SCAN ? slack + 2.0f * (float)(L + 1) * (float)(2 * M + 6 * VC + 64) * 5.9604645e-8f / kLn2 : slack;
+      if (!rows && bits_stat(fsc, r.filtersc) >= thr[r.p].s3 - sl) push_pair(r, bin, out, out_bins, out_counts, overflow);
     }
   }
 }

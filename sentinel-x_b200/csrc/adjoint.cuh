@@ -63,20 +63,33 @@ __device__ __forceinline__ float adj_fwd_row(const Img<VC>& img, int lane, int M
     a[c] = fmul(c ? mv[c - 1] : mcl, img.at(kRowFwd + 6, c, lane));
     pdd[c] = img.at(kRowFwd + 7, c, lane);
   }
-  float dcar = 0.f, xe = 0.f;
-  for (int sl = 0; sl < nl; sl++) {
-    if (lane == sl) {
+  // D chain D[k] = a_k + D[k-1] p_k as an affine scan across lanes, row sum as
+  // a butterfly (the adjoint is checked against FP64, not bit for bit)
+  float A = 0.f, B = 1.f;
 #pragma unroll
-      for (int c = 0; c < VC; c++) {
-        const float d = fadd(a[c], fmul(dcar, pdd[c]));
-        dv[c] = d;
-        xe = fadd(xe, fadd(mv[c], d));
-        dcar = d;
-      }
-    }
-    dcar = __shfl_sync(kFull, dcar, sl);
-    xe = __shfl_sync(kFull, xe, sl);
+  for (int c = 0; c < VC; c++) {
+    A = fadd(a[c], fmul(A, pdd[c]));
+    B = fmul(B, pdd[c]);
   }
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const float Au = __shfl_up_sync(kFull, A, o), Bu = __shfl_up_sync(kFull, B, o);
+    if (lane >= o) {
+      A = fadd(A, fmul(B, Au));
+      B = fmul(B, Bu);
+    }
+  }
+  const float din = __shfl_up_sync(kFull, A, 1);
+  float dcar = lane ? din : 0.f, xe = 0.f;
+#pragma unroll
+  for (int c = 0; c < VC; c++) {
+    const float d = fadd(a[c], fmul(dcar, pdd[c]));
+    dv[c] = d;
+    xe = fadd(xe, fadd(mv[c], d));
+    dcar = d;
+  }
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) xe = fadd(xe, __shfl_xor_sync(kFull, xe, o));
   if (lane >= nl) {
 #pragma unroll
     for (int c = 0; c < VC; c++) dv[c] = 0.f;
@@ -209,9 +222,9 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(const AdjPair* __
     const double* lsf = dbuf + A.ls_off;
     const double lz = lnz[w];
     const int W = M + 1;
-    float* o_msc = out + A.out_off;
-    float* o_isc = o_msc + 25 * W;
-    float* o_tr = o_isc + 25 * W;
+    float* __restrict__ o_msc = out + A.out_off;  // the three count arrays never overlap
+    float* __restrict__ o_isc = out + A.out_off + 25 * W;
+    float* __restrict__ o_tr = out + A.out_off + 50 * W;
     if (L <= 0 || !(lz > -INFINITY)) continue;
     const int rowf = 3 * 32 * VC;  // floats per stored row
     // Backward state: row i+1 (mn, inx, dn) and the specials
@@ -271,13 +284,10 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(const AdjPair* __
           pdd[c] = img.at(kRowBwd + 6, c, lane);
         }
         float b = 0.f;
-        for (int sl = 0; sl < nl; sl++) {
-          if (lane == sl) {
 #pragma unroll
-            for (int c = 0; c < VC; c++) b = fadd(b, bt[c]);
-          }
-          b = __shfl_sync(kFull, b, sl);
-        }
+        for (int c = 0; c < VC; c++) b = fadd(b, bt[c]);
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) b = fadd(b, __shfl_xor_sync(kFull, b, o));
         bxb = b;
         bxj = fadd(fmul(bxj, ploop), fmul(bxb, pmove));
         bxc = fmul(bxc, ploop);
@@ -291,24 +301,39 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(const AdjPair* __
           mnext[c] = c < VC - 1 ? me[c + 1] : (lane < 31 ? me_up : 0.f);
           iv[c] = fmul(inx[c], ins);
         }
-        float dcar = 0.f;
-        for (int sl = lM; sl >= 0; sl--) {
-          if (lane == sl) {
+        // D chain, descending: D[k] = (mnext_k p_dm + bxe) + p_dd D[k+1], D[M] = bxe,
+        // as an affine scan from the top lane down
+        float A = 0.f, B = 1.f;
 #pragma unroll
-            for (int c = VC - 1; c >= 0; c--) {
-              const int k = lane * VC + c + 1;
-              if (k > M) {
-                dc[c] = 0.f;
-              } else if (k == M) {
-                dc[c] = bxe;
-                dcar = bxe;
-              } else {
-                dc[c] = fadd(fadd(fmul(mnext[c], pdm[c]), fmul(dcar, pdd[c])), bxe);
-                dcar = dc[c];
-              }
-            }
+        for (int c = VC - 1; c >= 0; c--) {
+          const int k = lane * VC + c + 1;
+          const float al = k < M ? fadd(fmul(mnext[c], pdm[c]), bxe) : (k == M ? bxe : 0.f);
+          const float be = k < M ? pdd[c] : 0.f;
+          A = fadd(al, fmul(be, A));
+          B = fmul(be, B);
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const float Ad = __shfl_down_sync(kFull, A, o), Bd = __shfl_down_sync(kFull, B, o);
+          if (lane + o < 32) {
+            A = fadd(A, fmul(B, Ad));
+            B = fmul(B, Bd);
           }
-          dcar = __shfl_sync(kFull, dcar, sl);
+        }
+        const float dtop = __shfl_down_sync(kFull, A, 1);
+        float dcar = lane < 31 ? dtop : 0.f;
+#pragma unroll
+        for (int c = VC - 1; c >= 0; c--) {
+          const int k = lane * VC + c + 1;
+          if (k > M) {
+            dc[c] = 0.f;
+          } else if (k == M) {
+            dc[c] = bxe;
+            dcar = bxe;
+          } else {
+            dc[c] = fadd(fadd(fmul(mnext[c], pdm[c]), fmul(dcar, pdd[c])), bxe);
+            dcar = dc[c];
+          }
         }
         if (lane > lM) {
 #pragma unroll
@@ -371,9 +396,10 @@ __global__ void __launch_bounds__(128) adjoint_backward_kernel(const AdjPair* __
       // ---- accumulate counts ----
       const int x = __ldg(s + i - 1);
       const float fb0 = sp[6 * (i - 1) + 1];
-      const float f_ii = (float)exp(lsf[i] + lnsb_i - lz);        // F(i) . B(i)
-      const float f_i0 = (float)exp(lsf[i - 1] + lnsb_i - lz);    // F(i-1) . B(i)
-      const float f_i1 = (float)exp(lsf[i] + lnsb_next - lz);     // F(i) . B(i+1)
+      // scale factors of the scaled cell products, exponents formed in f64
+      const float f_ii = expf((float)(lsf[i] + lnsb_i - lz));        // F(i) . B(i)
+      const float f_i0 = expf((float)(lsf[i - 1] + lnsb_i - lz));    // F(i-1) . B(i)
+      const float f_i1 = expf((float)(lsf[i] + lnsb_next - lz));     // F(i) . B(i+1)
       const float fm0l0 = __shfl_up_sync(kFull, fm0[VC - 1], 1), fi0l0 = __shfl_up_sync(kFull, fi0[VC - 1], 1);
       const float fd0l0 = __shfl_up_sync(kFull, fd0[VC - 1], 1), fm1l0 = __shfl_up_sync(kFull, fm1[VC - 1], 1);
       const float fd1l0 = __shfl_up_sync(kFull, fd1[VC - 1], 1);

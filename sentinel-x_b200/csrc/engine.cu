@@ -112,6 +112,29 @@ struct DevBuf {
   }
 };
 
+// Page-locked host buffer (grow-only): device-to-host copies into it run at
+// full link speed and never fault in fresh pages.
+template <typename T>
+struct PinnedBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(const PinnedBuf&) = delete;
+  ~PinnedBuf() { release(); }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count <= n && p) return;
+    release();
+    CK(cudaHostAlloc((void**)&p, std::max<size_t>(count, 1) * sizeof(T), cudaHostAllocDefault));
+    n = std::max<size_t>(count, 1);
+  }
+};
+
 // ---- kernel shapes ---------------------------------------------------------
 // MSV (G lanes per target, C columns per lane) shapes compiled into the library.
 struct MsvShape {
@@ -528,6 +551,7 @@ struct sx_engine {
   DevBuf<int32_t> slots, plist;
   DevBuf<sxk::AdjPair> adj_pairs;
   DevBuf<float> adj_f, adj_out;
+  PinnedBuf<float> adj_host;  // staging of the adjoint's counts on their way to the caller
   DevBuf<double> adj_d, adj_lnz;
 };
 
@@ -2744,15 +2768,19 @@ int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, c
                                         t->d_len.p, t->d_xsc.p, e->adj_f.p, e->adj_d.p, e->adj_lnz.p, e->adj_out.p);
       CK(cudaGetLastError());
       // scatter the packed [25W | 25W | 8W] outputs straight into the caller's three arrays
-      const size_t sp = sizeof(float) * out_per;
-      CK(cudaMemcpy2DAsync(d_msc + i0 * 25 * W, sizeof(float) * 25 * W, e->adj_out.p, sp, sizeof(float) * 25 * W,
-                           (size_t)n, cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpy2DAsync(d_isc + i0 * 25 * W, sizeof(float) * 25 * W, e->adj_out.p + 25 * W, sp,
-                           sizeof(float) * 25 * W, (size_t)n, cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpy2DAsync(d_trans + i0 * 8 * W, sizeof(float) * 8 * W, e->adj_out.p + 50 * W, sp,
-                           sizeof(float) * 8 * W, (size_t)n, cudaMemcpyDeviceToHost, s));
+      // one copy into page-locked staging, then the host threads split the
+      // counts into the caller's three arrays (and fault in their pages)
+      e->adj_host.alloc(out_per * (size_t)n);
+      CK(cudaMemcpyAsync(e->adj_host.p, e->adj_out.p, sizeof(float) * out_per * (size_t)n, cudaMemcpyDeviceToHost, s));
       CK(cudaMemcpyAsync(lnz + i0, e->adj_lnz.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
+      const float* hs = e->adj_host.p;
+      parallel_for((size_t)n, e->host_threads, [&](size_t q) {
+        const float* src = hs + q * out_per;
+        memcpy(d_msc + (i0 + q) * 25 * W, src, sizeof(float) * 25 * W);
+        memcpy(d_isc + (i0 + q) * 25 * W, src + 25 * W, sizeof(float) * 25 * W);
+        memcpy(d_trans + (i0 + q) * 8 * W, src + 50 * W, sizeof(float) * 8 * W);
+      });
       i0 = i1;
     }
   } catch (const CudaError& ce) {

@@ -226,15 +226,26 @@ class Engine:
                                    p("msv"), p("viterbi"), p("forward"), p("backward"), p("bias")))
         return {s: v[:n] for s, v in out.items()}
 
-    def posterior_grad(self, profiles, targets, pp, pt, m):
+    def posterior_grad(self, profiles, targets, pp, pt, m, out=None):
+        """lnZ and its gradients for each pair (sx_posterior_grad).  `out`:
+        optional (lnz, d_msc, d_isc, d_tr) arrays to write into, of shapes (n,),
+        (n, 25, m+1), (n, 25, m+1), (n, 8, m+1), float64 then float32,
+        C-contiguous -- e.g. gradient buffers reused across calls, which spares
+        the page faults of fresh memory."""
         pp = np.ascontiguousarray(pp, dtype=np.int32)
         pt = np.ascontiguousarray(pt, dtype=np.int32)
         n = len(pp)
         w = m + 1
-        d_msc = np.zeros((n, 25, w), np.float32)
-        d_isc = np.zeros((n, 25, w), np.float32)
-        d_tr = np.zeros((n, 8, w), np.float32)
-        lnz = np.zeros(n, np.float64)
+        shapes = ((n,), (n, 25, w), (n, 25, w), (n, 8, w))
+        dtypes = (np.float64, np.float32, np.float32, np.float32)
+        if out is None:
+            lnz, d_msc, d_isc, d_tr = (np.empty(sh, dt) for sh, dt in zip(shapes, dtypes))
+        else:
+            for a, sh, dt in zip(out, shapes, dtypes):
+                if a.shape != sh or a.dtype != dt or not a.flags.c_contiguous or not a.flags.writeable:
+                    raise ValueError(f"posterior_grad: out array must be a writeable C-contiguous {np.dtype(dt)} "
+                                     f"array of shape {sh}")
+            lnz, d_msc, d_isc, d_tr = out
         _check(_lib.sx_posterior_grad(self.h, profiles.h, targets.h, _ptr(pp, C.c_int32), _ptr(pt, C.c_int32), n, m,
                                       _ptr(d_msc, C.c_float), _ptr(d_isc, C.c_float), _ptr(d_tr, C.c_float),
                                       _ptr(lnz, C.c_double)))

@@ -131,3 +131,18 @@ def test_adjoint_finite_differences_via_autograd(engine):
         for kind, idx, g in checks:
             fd = (o.forward_f64(pi, d, True, kind, idx, h) - o.forward_f64(pi, d, True, kind, idx, -h)) / (2 * h)
             assert abs(float(g) - fd) <= 1e-3 + 1e-3 * abs(fd), (pi, kind, idx, float(g), fd)
+
+
+def test_adjoint_out_arrays_reused(engine, adj_case):
+    """Gradients written into caller-provided (reused) arrays equal a fresh
+    call's; arrays of the wrong shape are refused."""
+    w = adj_case
+    pairs = w.pairs[:4]
+    ps, ts, fresh = _gpu(engine, w.hmm_text(), w.targets, pairs, 300)
+    out = tuple(np.full_like(a, np.nan) for a in fresh)
+    pp, pt = [a for a, _ in pairs], [b for _, b in pairs]
+    engine.posterior_grad(ps, ts, pp, pt, 300, out=out)
+    for a, b in zip(fresh, out):
+        assert np.array_equal(a, b)
+    with pytest.raises(ValueError):
+        engine.posterior_grad(ps, ts, pp, pt, 300, out=(out[0], out[1][:, :24], out[2], out[3]))

@@ -215,6 +215,19 @@ typedef struct {
 } sx_search_stats;
 int sx_last_search_stats(const sx_engine* e, sx_search_stats* out);
 
+/* ---- kernel shapes (for tuners) ------------------------------------------ */
+/* kind 0: MSV lane-group shapes (G lanes x C columns per lane); kind 1:
+ * Viterbi lane-group shapes (G, C, transitions held in registers).  A profile
+ * of M <= 2048 nodes runs with the shape the engine's table gives for M, else
+ * with the built-in choice.  sx_set_shape_table takes one entry per M =
+ * 0..2048 (-1 = the cost model; a shape must hold G*C >= M columns), or len
+ * = 0 to restore the built-in table (for Viterbi the shapes measured fastest
+ * per range of M on B200); it applies to profile sets loaded afterwards. */
+int sx_shape_count(int kind);
+int sx_shape_info(int kind, int index, int32_t* g, int32_t* c, int32_t* rt);
+int sx_shape_for(const sx_engine* e, int kind, int32_t m);
+int sx_set_shape_table(sx_engine* e, int kind, const int32_t* shape_by_m, size_t len);
+
 /* ---- stage scores for explicit pairs ----------------------------------- */
 /* Scores of msv (dp.rs:69), viterbi_score (dp.rs:152), forward (dp.rs:229),
  * backward (dp.rs:301) and bias_filter_score (pipeline.rs:107) for each pair

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "sxhmm", "libsxhmm.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 SOURCES = ["engine.cu", "hmmfile.cpp", "domains.cpp"]
-HEADERS = ["kernels.cuh", "adjoint.cuh", "plain.cuh", "long.cuh", "envelope.cuh", "internal.hpp"]
+HEADERS = ["kernels.cuh", "adjoint.cuh", "plain.cuh", "long.cuh", "envelope.cuh", "internal.hpp", "tuned_shapes.inc"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 

@@ -42,6 +42,7 @@
 #include "adjoint.cuh"
 #include "long.cuh"
 #include "envelope.cuh"
+#include "tuned_shapes.inc"
 
 using namespace sx;
 using sxk::BinRegion;
@@ -529,6 +530,9 @@ struct sx_engine {
   std::mutex mu;
   sx_search_stats stats{};
   int pipeline_blocks = 0;  // profile blocks per search; 0 = by workload size
+  // kernel shape per profile length, set by a tuner (sx_set_shape_table):
+  // [0] MSV, [1] Viterbi; empty or -1 = the built-in choice
+  std::vector<int16_t> shape_table[2];
   int64_t mem_free = 0;     // device memory free when the engine was created
   BlockPool target_blocks;  // device memory of freed target sets
   // envelope passes of the host domain definition (used by the host pool's
@@ -608,6 +612,31 @@ void join_aux(Streams& X) {
     CK(cudaEventRecord(X.join_ev[a], X.aux[a]));
     CK(cudaStreamWaitEvent(X.main, X.join_ev[a], 0));
   }
+}
+
+// The built-in shape table of a kind: for Viterbi the shapes measured fastest
+// per range of M on B200 (tuned_shapes.inc, written by sxhmm/tune.py); none for
+// MSV, whose cost model was fitted to ncu instruction counts.
+std::vector<int16_t> default_shape_table(int kind) {
+  std::vector<int16_t> t;
+  if (kind != 1) return t;
+  t.assign(kMaxM + 1, -1);
+  for (const auto& r : kTunedVit) {
+    int idx = -1;
+    for (int s = 0; s < kNumVitShapes; s++)
+      if (kVitShapes[s].g == r[2] && kVitShapes[s].c == r[3] && kVitShapes[s].rt == r[4]) idx = s;
+    if (idx < 0 || kVitShapes[idx].g * kVitShapes[idx].c < r[1]) continue;
+    for (int m = std::max(r[0], 0); m <= r[1] && m <= kMaxM; m++) t[(size_t)m] = (int16_t)idx;
+  }
+  return t;
+}
+
+// Kernel shape for a profile of length m: the engine's table where it has an
+// entry, else the cost model (kind 0 MSV, 1 Viterbi).
+int shape_for(const sx_engine* E, int kind, int m) {
+  const auto& t = E->shape_table[kind];
+  if (m >= 0 && (size_t)m < t.size() && t[(size_t)m] >= 0) return t[(size_t)m];
+  return kind == 0 ? choose_msv_shape(m) : choose_vit_shape(m);
 }
 
 // ---- profile packing --------------------------------------------------------
@@ -746,7 +775,7 @@ void pack_profiles(sx_profiles* P) {
       d.vit_off = vit_total;
       continue;
     }
-    const int s = choose_msv_shape(h.m);
+    const int s = shape_for(P->eng, 0, h.m);
     const int vb = choose_vbin(h.m);
     if (s < 0 || vb < 0) throw CudaError{SX_EINVAL, "profile '" + h.name + "': no kernel shape for M=" + std::to_string(h.m)};
     P->msv_shape[i] = s;
@@ -758,7 +787,7 @@ void pack_profiles(sx_profiles* P) {
     msv_total += 25LL * (d.msv_c / 4) * d.msv_g;
     d.vfb_off = vfb_total;
     vfb_total += (int64_t)sxk::kImgRows * 32 * d.vc;
-    d.vshape = choose_vit_shape(h.m);
+    d.vshape = shape_for(P->eng, 1, h.m);
     if (d.vshape < 0) throw CudaError{SX_EINVAL, "profile '" + h.name + "' too long for the Viterbi shapes"};
     d.vit_off = vit_total;
     vit_total += 33LL * (kVitShapes[d.vshape].c / 4) * kVitShapes[d.vshape].g;
@@ -2251,6 +2280,7 @@ int sx_create(const sx_opts* opts, sx_engine** out) {
       CK(cudaEventCreateWithFlags(&e->env_ev, cudaEventDisableTiming));
     }
     note_free_memory(e.get());
+    for (int kind = 0; kind < 2; kind++) e->shape_table[kind] = default_shape_table(kind);
     (void)kernels();
   } catch (const CudaError& ce) {
     return fail(ce.code, ce.msg);
@@ -2553,6 +2583,48 @@ size_t sx_hits_domain_count(const sx_hits* h) { return h ? h->doms.size() : 0; }
 const sx_domain* sx_hits_domains(const sx_hits* h) { return h && !h->doms.empty() ? h->doms.data() : nullptr; }
 void sx_hits_free(sx_hits* h) { delete h; }
 
+int sx_shape_count(int kind) { return kind == 0 ? kNumMsvShapes : kind == 1 ? kNumVitShapes : -1; }
+
+int sx_shape_info(int kind, int index, int32_t* g, int32_t* c, int32_t* rt) {
+  if (kind < 0 || kind > 1 || index < 0 || index >= sx_shape_count(kind) || !g || !c || !rt)
+    return fail(SX_EINVAL, "sx_shape_info: bad kind or index");
+  if (kind == 0) {
+    *g = kMsvShapes[index].g;
+    *c = kMsvShapes[index].c;
+    *rt = 0;
+  } else {
+    *g = kVitShapes[index].g;
+    *c = kVitShapes[index].c;
+    *rt = kVitShapes[index].rt;
+  }
+  return SX_OK;
+}
+
+int sx_shape_for(const sx_engine* e, int kind, int32_t m) {
+  if (!e || kind < 0 || kind > 1 || m < 0) return -1;
+  return is_long(m) ? -1 : shape_for(e, kind, m);
+}
+
+int sx_set_shape_table(sx_engine* e, int kind, const int32_t* shape_by_m, size_t len) {
+  if (!e || kind < 0 || kind > 1 || (len && !shape_by_m)) return fail(SX_EINVAL, "sx_set_shape_table: bad argument");
+  if (len != 0 && len != (size_t)kMaxM + 1)
+    return fail(SX_EINVAL, "sx_set_shape_table: the table has one entry per M = 0.." + std::to_string(kMaxM));
+  std::vector<int16_t> t = len ? std::vector<int16_t>(len, -1) : default_shape_table(kind);
+  for (size_t m = 0; m < len; m++) {
+    const int s = shape_by_m[m];
+    if (s < 0) continue;
+    if (s >= sx_shape_count(kind)) return fail(SX_EINVAL, "sx_set_shape_table: shape " + std::to_string(s) + " unknown");
+    const int cols = kind == 0 ? kMsvShapes[s].g * kMsvShapes[s].c : kVitShapes[s].g * kVitShapes[s].c;
+    if (cols < (int)m)
+      return fail(SX_EINVAL, "sx_set_shape_table: shape " + std::to_string(s) + " holds " + std::to_string(cols) +
+                                 " columns, fewer than M=" + std::to_string(m));
+    t[m] = (int16_t)s;
+  }
+  std::lock_guard<std::mutex> lk(e->mu);
+  e->shape_table[kind] = std::move(t);
+  return SX_OK;
+}
+
 int sx_last_search_stats(const sx_engine* e, sx_search_stats* out) {
   if (!e || !out) return fail(SX_EINVAL, "sx_last_search_stats: NULL argument");
   *out = e->stats;
@@ -2659,6 +2731,7 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
       if (viterbi) {
         e->sl[0].cursor.alloc(kMaxBins);
         CK(cudaMemsetAsync(e->sl[0].cursor.p, 0, sizeof(unsigned) * kMaxBins, s));
+        CK(cudaEventRecord(e->ev[0], s));
         for (int b = 0; b < kNumVitShapes; b++) {
           if (!cnt[b]) continue;
           const int blocks = vit_blocks(e->num_sms, b, cnt[b]);
@@ -2667,8 +2740,12 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
                                            t->d_len.p, t->d_xsc.p, 0.f, e->scores.p, e->sl[0].cursor.p);
         }
         CK(cudaGetLastError());
+        CK(cudaEventRecord(e->ev[1], s));
         CK(cudaMemcpyAsync(viterbi, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
+        e->stats.ms[2] = elapsed_ms(e->ev[0], e->ev[1]);  // the Viterbi launches, for tuners
+        for (size_t i = 0; i < npairs; i++)
+          if (!is_long(p->h[pair_profile[i]].m)) e->stats.cells[2] += (double)p->h[pair_profile[i]].m * t->len[pair_target[i]];
         if (!lng.empty()) {
           std::vector<float> v;
           long_scores(e, p, t, lpairs, true, v);

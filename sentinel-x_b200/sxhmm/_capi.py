@@ -95,6 +95,10 @@ SIGNATURES = {
     "sx_hits_domains": (C.POINTER(SxDomain), [_P]),
     "sx_hits_free": (None, [_P]),
     "sx_last_search_stats": (C.c_int, [_P, C.POINTER(SxSearchStats)]),
+    "sx_shape_count": (C.c_int, [C.c_int]),
+    "sx_shape_info": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "sx_shape_for": (C.c_int, [_P, C.c_int, C.c_int32]),
+    "sx_set_shape_table": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int32), C.c_size_t]),
     "sx_score_pairs": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, _fp, _fp, _fp, _fp, _fp]),
     "sx_posterior_grad": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, C.c_int32, _fp, _fp, _fp, _dp]),
     "sx_score_viterbi_static": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, _fp]),
@@ -207,6 +211,31 @@ class Engine:
     def load_binary(self, path):
         """Profiles from a cache written by Profiles.save (sx_profiles_load_binary)."""
         return Profiles(self, binary=path)
+
+    # kernel shapes, for tuners: kind "msv" or "viterbi"
+    _KINDS = {"msv": 0, "viterbi": 1}
+
+    def shapes(self, kind):
+        """The compiled shapes of `kind` as (G, C, register transitions)."""
+        k = self._KINDS[kind]
+        out = []
+        for i in range(_lib.sx_shape_count(k)):
+            g, c, rt = C.c_int32(), C.c_int32(), C.c_int32()
+            _check(_lib.sx_shape_info(k, i, C.byref(g), C.byref(c), C.byref(rt)))
+            out.append((g.value, c.value, rt.value))
+        return out
+
+    def shape_for(self, kind, m):
+        return _lib.sx_shape_for(self.h, self._KINDS[kind], int(m))
+
+    def set_shape_table(self, kind, table):
+        """Shape index per M = 0..2048 (-1 = the cost model), or None to
+        restore the built-in table; applies to profile sets loaded afterwards."""
+        if table is None:
+            _check(_lib.sx_set_shape_table(self.h, self._KINDS[kind], None, 0))
+            return
+        t = np.ascontiguousarray(table, dtype=np.int32)
+        _check(_lib.sx_set_shape_table(self.h, self._KINDS[kind], _ptr(t, C.c_int32), len(t)))
 
     def stats(self):
         s = SxSearchStats()

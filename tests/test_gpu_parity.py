@@ -209,6 +209,28 @@ def test_long_profiles(engine):
         engine.posterior_grad(ps, ts, np.array([0], np.int32), np.array([5], np.int32), 2100)
 
 
+def test_shape_table_same_hits():
+    """A tuner's shape table (sx_set_shape_table) changes only the kernel
+    shapes: with every profile on the widest Viterbi shape, or on the tuned
+    ones, the hits equal the oracle's; a shape too narrow for M is refused."""
+    w = small_config(1, 0.01)
+    seqs = [(w.target_ids[i], _decode(s)) for i, s in enumerate(w.targets)]
+    e = sxhmm.Engine()
+    try:
+        shapes = e.shapes("viterbi")
+        widest = max(range(len(shapes)), key=lambda i: shapes[i][0] * shapes[i][1])
+        e.set_shape_table("viterbi", np.full(2049, widest, np.int32))
+        assert e.shape_for("viterbi", 150) == widest
+        _cmp(e, w.hmm_text(), seqs, filters=True)
+        narrow = min(range(len(shapes)), key=lambda i: shapes[i][0] * shapes[i][1])
+        with pytest.raises(sxhmm.HmmError, match="fewer than M"):
+            e.set_shape_table("viterbi", np.full(2049, narrow, np.int32))
+        e.set_shape_table("viterbi", None)
+        _cmp(e, w.hmm_text(), seqs, filters=True)
+    finally:
+        e.close()
+
+
 def test_missing_cutoff_raises_like_reference(engine):
     ps = engine.load_text(tiny_text())
     with pytest.raises(sxhmm.HmmError, match="TC bit thresholds unavailable on model tiny"):

@@ -395,6 +395,37 @@ float f32_boundary(Pred pass) {
 // Device blocks recycled between target sets, so that a caller streaming
 // batches of targets through one engine does not pay a cudaMalloc/cudaFree
 // pair (and the device-wide synchronisation of cudaFree) per batch.
+// Host buffers of packed residues, recycled across target sets so that a
+// caller streaming batches of targets writes into pages already touched.
+class HostBytePool {
+ public:
+  std::vector<uint8_t> take(size_t bytes) {
+    std::lock_guard<std::mutex> g(mu_);
+    for (size_t i = 0; i < free_.size(); i++)
+      if (free_[i].capacity() >= bytes) {
+        std::vector<uint8_t> v = std::move(free_[i]);
+        free_.erase(free_.begin() + (std::ptrdiff_t)i);
+        v.clear();
+        return v;
+      }
+    std::vector<uint8_t> v;
+    v.reserve(bytes);
+    return v;
+  }
+  void give(std::vector<uint8_t>&& v) {
+    if (!v.capacity()) return;
+    std::lock_guard<std::mutex> g(mu_);
+    free_.push_back(std::move(v));
+    if (free_.size() > 2)  // keep the two largest
+      free_.erase(std::min_element(free_.begin(), free_.end(),
+                                   [](const auto& x, const auto& y) { return x.capacity() < y.capacity(); }));
+  }
+
+ private:
+  std::mutex mu_;
+  std::vector<std::vector<uint8_t>> free_;
+};
+
 class BlockPool {
  public:
   ~BlockPool() {
@@ -535,6 +566,7 @@ struct sx_engine {
   std::vector<int16_t> shape_table[2];
   int64_t mem_free = 0;     // device memory free when the engine was created
   BlockPool target_blocks;  // device memory of freed target sets
+  HostBytePool target_bytes;  // host residue buffers of freed target sets
   // envelope passes of the host domain definition (used by the host pool's
   // driver thread, one batch at a time)
   cudaStream_t env_stream = nullptr, env_stream2 = nullptr;  // Backward runs beside Forward
@@ -591,6 +623,7 @@ struct sx_targets {
   size_t block_bytes = 0;
   ~sx_targets() {
     if (block) eng->target_blocks.give(block, block_bytes);
+    eng->target_bytes.give(std::move(dsq));
   }
 };
 
@@ -858,9 +891,20 @@ void pack_targets(sx_targets* T) {
     xsc[i] = it->second.second;
     T->residues += (double)l;
   }
+  // indices by length, longest first, ties in input order (a counting sort
+  // when the lengths allow one)
   T->order.resize(n);
-  std::iota(T->order.begin(), T->order.end(), 0);
-  std::stable_sort(T->order.begin(), T->order.end(), [&](int a, int b) { return T->len[a] > T->len[b]; });
+  int32_t mx = 0;
+  for (size_t i = 0; i < n; i++) mx = std::max(mx, T->len[i]);
+  if (mx <= (1 << 22)) {
+    std::vector<int32_t> start((size_t)mx + 2, 0);
+    for (size_t i = 0; i < n; i++) start[(size_t)(mx - T->len[i]) + 1]++;
+    for (size_t k = 1; k < start.size(); k++) start[k] += start[k - 1];
+    for (size_t i = 0; i < n; i++) T->order[(size_t)start[(size_t)(mx - T->len[i])]++] = (int32_t)i;
+  } else {
+    std::iota(T->order.begin(), T->order.end(), 0);
+    std::stable_sort(T->order.begin(), T->order.end(), [&](int a, int b) { return T->len[a] > T->len[b]; });
+  }
   cudaStream_t s = T->eng->stream;
   // all arrays in one pooled block, each 256-byte aligned
   auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
@@ -2449,6 +2493,9 @@ int sx_targets_create(sx_engine* e, const char* const* ids, const uint8_t* const
   std::lock_guard<std::mutex> lk(e->mu);
   auto t = std::make_unique<sx_targets>();
   t->eng = e;
+  size_t total = 64;  // an upper bound of the packed size
+  for (size_t i = 0; i < n; i++) total += (lens[i] + 15) & ~(size_t)15;
+  t->dsq = e->target_bytes.take(total);
   std::vector<uint8_t> dig;
   for (size_t i = 0; i < n; i++) {
     dig.clear();
@@ -2476,7 +2523,7 @@ int sx_targets_create_digital(sx_engine* e, const uint8_t* dsq, const int64_t* o
     if (lens[i] < 0 || offsets[i] < 0 || lens[i] > INT32_MAX) return fail(SX_EINVAL, "sx_targets_create_digital: bad length");
     total += ((size_t)lens[i] + 15) & ~(size_t)15;
   }
-  t->dsq.reserve(total);
+  t->dsq = e->target_bytes.take(total);
   t->off.reserve(n);
   t->len.reserve(n);
   for (size_t i = 0; i < n; i++) {

@@ -231,6 +231,18 @@ def test_shape_table_same_hits():
         e.close()
 
 
+def test_empty_inputs(engine):
+    """No profiles (an empty HMM text) or no targets: no hits and no error,
+    as the reference's reader and search give."""
+    assert _hits_gpu(engine, "", [("a", "MKAGG")], {}) == _hits_oracle("", [("a", "MKAGG")], O.make_cfg()) == []
+    cfg = {"cutoff": "T", "seq": -1e9, "dom": -1e9, "filters": False}
+    assert _hits_gpu(engine, tiny_text(), [], cfg) == []
+    ps = engine.load_text(tiny_text())
+    ts = engine.targets(["MKA"])
+    got = engine.score_pairs(ps, ts, np.zeros(0, np.int32), np.zeros(0, np.int32))
+    assert all(len(v) <= 1 for v in got.values())
+
+
 def test_missing_cutoff_raises_like_reference(engine):
     ps = engine.load_text(tiny_text())
     with pytest.raises(sxhmm.HmmError, match="TC bit thresholds unavailable on model tiny"):

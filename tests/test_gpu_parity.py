@@ -207,6 +207,18 @@ def test_long_profiles(engine):
     ts = engine.targets([q[1] for q in seqs if q[1]])
     with pytest.raises(sxhmm.HmmError, match="M > 2048"):
         engine.posterior_grad(ps, ts, np.array([0], np.int32), np.array([5], np.int32), 2100)
+    # the plain engine and sx_search_many take the same long-profile pass
+    plain = sxhmm.Engine(plain=True)
+    try:
+        _assert_same_hits(_hits_oracle(text, seqs, O.make_cfg()), _hits_gpu(plain, text, seqs, {}))
+    finally:
+        plain.close()
+    sets = [engine.load_text(part + "//\n") for part in text.split("//\n") if part.strip()]
+    cfg = sxhmm.SearchConfig().to_c()
+    many = engine.search_many(sets, ts, cfg)
+    for st, got in zip(sets, many):
+        assert _raw(got) == _raw(engine.search(st, ts, cfg))
+    assert sum(len(h) for h, _ in many) > 0
 
 
 def test_shape_table_same_hits():

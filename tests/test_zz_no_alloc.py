@@ -17,7 +17,7 @@ import pytest
 
 import sxhmm
 from sxhmm import _capi
-from _workloads import edge_targets, fixture_targets, fixture_text, small_profiles_text, tiny_text
+from _workloads import edge_targets, fixture_targets, fixture_text, long_workload, small_profiles_text, tiny_text
 
 pytestmark = pytest.mark.gpu
 
@@ -52,5 +52,10 @@ def test_static_matches_score_pairs_twice():
             assert np.array_equal(got, want), (call, np.nonzero(got != want)[0][:5])
         with pytest.raises(sxhmm.HmmError, match="exceed the fixed limit"):
             _static_scores(eng, ps, ts, np.zeros(8193, np.int32), np.zeros(8193, np.int32))
+        text_long, seqs_long = long_workload()
+        pl = eng.load_text(text_long)
+        tl = eng.targets([s for _, s in seqs_long if s])
+        with pytest.raises(sxhmm.HmmError, match="M > 2048"):
+            _static_scores(eng, pl, tl, np.zeros(1, np.int32), np.zeros(1, np.int32))
     finally:
         eng.close()

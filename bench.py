@@ -447,6 +447,10 @@ def main():
     achieved = MSV_OPS_PER_CELL * statistics.median(msv_cells) / msv_t / 1e12
     sm_mhz = clocks.get("sm_mhz") or 1965.0
     peak = 148 * 128 * sm_mhz * 1e6 / 1e12  # FP32 lanes x SMs x sampled SM clock
+    # the kernel's second ceiling: every DP cell reads its 4-byte emission score
+    # from shared memory, 128 bytes per clock per SM
+    smem_achieved = 4.0 * statistics.median(msv_cells) / msv_t / 1e12
+    smem_peak = 148 * 128 * sm_mhz * 1e6 / 1e12
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "msv_traffic.json")
     if os.path.exists(tfile):
@@ -468,6 +472,10 @@ def main():
                          "measured_in": "single-block search (pipeline_blocks=1): MSV launches alone on the GPU, "
                                         "CUDA events around them",
                          "single_block_ms_per_step": round(max(single_ms), 3)},
+            "roofline_shared": {"bound": "shared memory", "kernel": "msv_kernel", "achieved": smem_achieved,
+                                "peak": smem_peak, "unit": "TB/s", "frac": smem_achieved / smem_peak,
+                                "note": "4 B of emission score read from shared memory per DP cell; peak 128 B per "
+                                        "clock per SM x 148 SMs x median sampled SM clock"},
             "stage_ms": {k: round(v / max(1, args.steps), 3) for k, v in zip(STAGES, stage_ms)},
             "stage_pairs_in": dict(zip(["msv", "bias", "viterbi", "forward", "rows", "host_domains"], stage_pairs or [])),
             "stage_gcups": stage_gcups, "stage_cells": stage_cells,

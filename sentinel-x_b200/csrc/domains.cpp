@@ -134,6 +134,20 @@ struct Sample {  // p7_spcoord_s
   int k, m;
 };
 
+// Full-matrix workspaces of envelope rescoring: one set per thread, reused by
+// every EnvelopeScorer the thread creates (a fresh set per pair faulted in
+// megabytes of new pages every time).  Each use re-initialises what it reads,
+// and a thread runs one scorer at a time.
+struct ScorerWork {
+  Mat fx, bx;
+  Post pp;
+  std::vector<float> om, oi, od;
+};
+ScorerWork& scorer_work() {
+  thread_local ScorerWork w;
+  return w;
+}
+
 class EnvelopeScorer {
  public:
   EnvelopeScorer(const ProfileHost& p, const uint8_t* dsq, int64_t l, const SearchOpts& o)
@@ -863,9 +877,13 @@ class EnvelopeScorer {
   const int64_t l_;
   const SearchOpts& o_;
   const size_t w_;
-  Mat fx_, bx_;
-  Post pp_;
-  std::vector<float> om_, oi_, od_;
+  ScorerWork& ws_ = scorer_work();
+  Mat& fx_ = ws_.fx;
+  Mat& bx_ = ws_.bx;
+  Post& pp_ = ws_.pp;
+  std::vector<float>& om_ = ws_.om;
+  std::vector<float>& oi_ = ws_.oi;
+  std::vector<float>& od_ = ws_.od;
 };
 
 // Log-space rows from the device's raw scaled rows.  Forward rows: slots

@@ -262,8 +262,10 @@ int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, c
  * synchronisation a cudaMalloc/cudaFree can imply.  Instead of engine scratch
  * it uses one fixed device array of about 360 KB that every GPU holding this
  * library keeps reserved until the process exits.  The first call on a device
- * looks up that array's device address; make that first call before any
- * stream capture begins on the device.  More than 8192 pairs is an SX_EINVAL
+ * looks up that array's device address (and the first call after the device's
+ * context was replaced, e.g. by cudaDeviceReset, looks it up again); make that
+ * first call before any stream capture begins on the device.  Profiles and
+ * targets must belong to the engine passed (SX_EINVAL otherwise).  More than 8192 pairs is an SX_EINVAL
  * error.  All calls on a device share the array: calls that overlap on the
  * GPU (for example from two engines on one device) race; calls on one engine
  * are serialised.  Inputs and outputs are host arrays, as for sx_score_pairs. */

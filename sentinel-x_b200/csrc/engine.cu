@@ -2682,6 +2682,7 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
                    const int32_t* pair_target, size_t npairs, float* msv, float* viterbi, float* forward,
                    float* backward, float* bias) {
   if (!e || !p || !t || (npairs && (!pair_profile || !pair_target))) return fail(SX_EINVAL, "sx_score_pairs: NULL argument");
+  if (p->eng != e || t->eng != e) return fail(SX_EINVAL, "sx_score_pairs: profiles/targets belong to another engine");
   std::lock_guard<std::mutex> lk(e->mu);
   NvtxRange nv("sx_score_pairs");
   const size_t np = p->h.size(), nt = t->len.size();
@@ -2831,6 +2832,7 @@ int sx_posterior_grad(sx_engine* e, const sx_profiles* p, const sx_targets* t, c
                       float* d_trans, double* lnz) {
   if (!e || !p || !t || (npairs && (!pair_profile || !pair_target || !d_msc || !d_isc || !d_trans || !lnz)))
     return fail(SX_EINVAL, "sx_posterior_grad: NULL argument");
+  if (p->eng != e || t->eng != e) return fail(SX_EINVAL, "sx_posterior_grad: profiles/targets belong to another engine");
   std::lock_guard<std::mutex> lk(e->mu);
   const size_t np = p->h.size(), nt = t->len.size();
   for (size_t i = 0; i < npairs; i++) {
@@ -2971,21 +2973,61 @@ __global__ void static_bucket_kernel(unsigned char* scratch, int npairs, const D
 }
 
 // Device address of g_static_scratch for each device, looked up once per
-// device (with that device current) on its first call.
+// device context (with that device current): on the first call on the device,
+// and again after the device's context has been replaced (cudaDeviceReset
+// destroys the primary context and the module that holds the array, so an
+// address cached before it would dangle).  The context is told apart by the
+// driver's context id, reached through the runtime's driver entry points so
+// the library needs no link to libcuda.
 std::mutex g_static_mu;
-void* g_static_ptr[128] = {};
+struct StaticAddr {
+  void* ptr = nullptr;
+  unsigned long long ctx_id = 0;
+};
+StaticAddr g_static_addr[128];
+
+typedef int (*CtxGetCurrentFn)(void** ctx);
+typedef int (*CtxGetIdFn)(void* ctx, unsigned long long* id);
+
+// Id of the calling thread's current context, or 0 when the driver cannot
+// report one (the cached address is then kept for the process lifetime).
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    cudaGetLastError();
+  });
+  if (!get_current || !get_id) return 0;
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 int static_scratch_ptr(int device, unsigned char** out) {
   if (device < 0 || device >= 128) return fail(SX_EINVAL, "sx_score_viterbi_static: device ordinal out of range");
   std::lock_guard<std::mutex> lk(g_static_mu);
-  if (!g_static_ptr[device]) {
+  StaticAddr& a = g_static_addr[device];
+  const unsigned long long ctx = current_context_id();
+  if (!a.ptr || ctx != a.ctx_id) {
     void* ptr = nullptr;
     const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_static_scratch);
     if (rc != cudaSuccess || !ptr)
       return fail(SX_ECUDA, std::string("sx_score_viterbi_static: cudaGetSymbolAddress: ") + cudaGetErrorString(rc));
-    g_static_ptr[device] = ptr;
+    a.ptr = ptr;
+    a.ctx_id = ctx;
   }
-  *out = static_cast<unsigned char*>(g_static_ptr[device]);
+  *out = static_cast<unsigned char*>(a.ptr);
   return SX_OK;
 }
 
@@ -2996,6 +3038,8 @@ extern "C" int sx_score_viterbi_static(sx_engine* e, const sx_profiles* p, const
                                        float* viterbi) {
   if (!e || !p || !t || (npairs && (!pair_profile || !pair_target || !viterbi)))
     return fail(SX_EINVAL, "sx_score_viterbi_static: NULL argument");
+  if (p->eng != e || t->eng != e)
+    return fail(SX_EINVAL, "sx_score_viterbi_static: profiles/targets belong to another engine");
   if (npairs > kStaticMaxPairs)
     return fail(SX_EINVAL, "sx_score_viterbi_static: " + std::to_string(npairs) + " pairs exceed the fixed limit of " +
                                std::to_string(kStaticMaxPairs) + " per call");

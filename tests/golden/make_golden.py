@@ -20,7 +20,8 @@ import os
 import shutil
 import sys
 
-REF = os.environ.get("SX_REFERENCE", "/root/reference")
+# The reference checkout to copy from, e.g. SX_REFERENCE=/path/to/sentinel-x
+REF = os.environ.get("SX_REFERENCE", "")
 SRC = os.path.join(REF, "src", "hmmer", "testdata")
 HERE = os.path.dirname(os.path.abspath(__file__))
 FILES = ["hmmer34_pair.hmm", "hmmer34_targets.faa", "hmmer34_expected.tsv", "tiny.hmm"]
@@ -59,6 +60,8 @@ UNIT = {
 
 
 def main():
+    if not REF:
+        sys.exit("set SX_REFERENCE to the reference checkout (the directory holding src/hmmer/testdata)")
     if not os.path.isdir(SRC):
         sys.exit(f"reference testdata not found at {SRC}")
     manifest = {}

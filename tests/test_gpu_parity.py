@@ -409,7 +409,10 @@ def test_search_edges(engine):
 
 @pytest.mark.parametrize("cutoff", ["E", "GA", "NC", "TC"])
 def test_search_synthetic_config0(engine, cutoff):
-    w = small_config(0, 0.2)
+    """The CPU-runnable configuration at full size: 1 profile of M = 100
+    against 1,000 targets (L 100-500, 5% planted homologs), filters on."""
+    w = small_config(0, 1.0)
+    assert len(w.targets) == 1000 and w.profiles[0].m == 100
     seqs = [(w.target_ids[i], "".join("ACDEFGHIKLMNPQRSTVWY"[x] for x in s)) for i, s in enumerate(w.targets)]
     a, b = _cmp(engine, w.hmm_text(), seqs, cutoff=cutoff, filters=True)
     if cutoff == "E":  # every planted homolog is reported

@@ -54,6 +54,11 @@ extern "C" {
  * Results are identical either way. */
 #define SX_FLAG_TRACE_HOST 8u    /* always on the host */
 #define SX_FLAG_TRACE_DEVICE 16u /* always on the device (with the envelopes) */
+/* MSV runs as a packed int16x2 pre-screen (an upper bound of the f32 score for
+ * two profiles per 32-bit lane) followed by the exact f32 MSV of the pairs whose
+ * bound passes F1; this flag runs the exact kernel on every pair instead.
+ * Results are identical either way. */
+#define SX_FLAG_NO_PRESCREEN 32u
 
 typedef struct sx_engine sx_engine;
 typedef struct sx_profiles sx_profiles;
@@ -118,7 +123,10 @@ typedef struct {
 } sx_profile_info;
 
 /* ---- engine ------------------------------------------------------------ */
-/* New: one engine per device. */
+/* New: one engine per device.  sx_destroy releases the engine's streams at
+ * once; profile and target sets of the engine may still be freed afterwards
+ * (the engine's memory goes when its last set does), but no other call may
+ * name the engine or its sets after sx_destroy. */
 int sx_create(const sx_opts* opts, sx_engine** out);
 void sx_destroy(sx_engine* e);
 /* Message of the last error on this thread ("" if none). */
@@ -212,6 +220,11 @@ typedef struct {
   double cells[8];
   double ms[8];
   int64_t kernel_launches;
+  /* the packed MSV pre-screen (part of stage 0): pairs it bounded, pairs
+   * whose bound passed F1 (rescored exactly), its DP cells, the device time
+   * of the pre-screen and of the exact rescoring */
+  int64_t prescreen_pairs_in, prescreen_pairs_out;
+  double prescreen_cells, prescreen_ms, rescore_ms;
 } sx_search_stats;
 int sx_last_search_stats(const sx_engine* e, sx_search_stats* out);
 
@@ -236,6 +249,23 @@ int sx_set_shape_table(sx_engine* e, int kind, const int32_t* shape_by_m, size_t
 int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, const int32_t* pair_profile,
                    const int32_t* pair_target, size_t npairs, float* msv, float* viterbi, float* forward,
                    float* backward, float* bias);
+
+/* ---- pre-screen bounds for explicit pairs (diagnostics) ------------------ */
+/* No counterpart in the reference: the two conservative screens the device
+ * cascade runs in front of exact stages, for tests and tuning.
+ *   msv_bound: the packed int16x2 MSV pre-screen's upper bound of the f32 MSV
+ *     score (nats; +inf when the pair hit the int16 headroom cap and passes
+ *     unconditionally).  It is >= the msv score of sx_score_pairs for every
+ *     pair; NaN for profiles the pre-screen does not handle (M > 2048, or
+ *     match scores above +16 nats).
+ *   fwd_scan: the F3 pre-screen's Forward score (nats), evaluated in a
+ *     parallel order that differs from the reference's; its difference from
+ *     the exact Forward score is bounded by (L+1)(2M + 6 VC + 64) 2^-24 nats,
+ *     taken twice (VC = columns per lane of the profile's warp-chunked image);
+ *     NaN for M > 2048.
+ * Either output pointer may be NULL to skip that screen. */
+int sx_score_prescreens(sx_engine* e, const sx_profiles* p, const sx_targets* t, const int32_t* pair_profile,
+                        const int32_t* pair_target, size_t npairs, float* msv_bound, float* fwd_scan);
 
 /* ---- adjoint ----------------------------------------------------------- */
 /* Gradient of each pair's Forward log score lnZ (multihit, target-length

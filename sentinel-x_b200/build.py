@@ -15,17 +15,32 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "sxhmm", "libsxhmm.so")
+OBJ = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
-SOURCES = ["engine.cu", "hmmfile.cpp", "domains.cpp"]
-HEADERS = ["kernels.cuh", "adjoint.cuh", "plain.cuh", "long.cuh", "envelope.cuh", "internal.hpp", "tuned_shapes.inc"]
+# the kernel instantiations sit in their own translation units so they
+# compile in parallel
+SOURCES = ["engine.cu", "k_msv.cu", "k_msv16.cu", "k_vit.cu", "k_vbin.cu", "k_env.cu", "hmmfile.cpp", "domains.cpp"]
+HEADERS = ["kernels.cuh", "adjoint.cuh", "plain.cuh", "long.cuh", "envelope.cuh", "internal.hpp", "shapes.hpp", "prescreen.cuh",
+           "tuned_shapes.inc"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 
-def cmd():
+def common():
     return [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
             "-Xptxas", "-v" if os.environ.get("SX_PTXAS_VERBOSE") else "-O3",
-            "-Xcompiler", "-fPIC,-O3,-ffp-contract=off,-fno-fast-math", "-shared", "-I", INCLUDE,
-            "-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lz", "-lpthread"]
+            "-Xcompiler", "-fPIC,-O3,-ffp-contract=off,-fno-fast-math", "-I", INCLUDE]
+
+
+def obj_of(src):
+    return os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
+
+
+def compile_cmd(src):
+    return common() + ["-c", os.path.join(CSRC, src), "-o", obj_of(src)]
+
+
+def link_cmd():
+    return common() + ["-shared", "-o", OUT] + [obj_of(s) for s in SOURCES] + ["-lz", "-lpthread"]
 
 
 def stale():
@@ -36,16 +51,27 @@ def stale():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _run(c):
+    r = subprocess.run(c, capture_output=True, text=True)
+    return r.returncode, r.stdout + r.stderr
+
+
 def build(force=False):
     if not force and not stale():
         return OUT
-    c = cmd()
-    r = subprocess.run(c, capture_output=True, text=True)
-    if r.returncode != 0:
-        sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libsxhmm.so")
-    if os.environ.get("SX_PTXAS_VERBOSE"):
-        sys.stderr.write(r.stderr)
+    from concurrent.futures import ThreadPoolExecutor
+    os.makedirs(OBJ, exist_ok=True)
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(_run, [compile_cmd(s) for s in SOURCES]))
+    for src, (rc, out) in zip(SOURCES, results):
+        if rc != 0 or os.environ.get("SX_PTXAS_VERBOSE"):
+            sys.stderr.write(out)
+        if rc != 0:
+            raise RuntimeError(f"nvcc failed compiling {src}")
+    rc, out = _run(link_cmd())
+    if rc != 0:
+        sys.stderr.write(out)
+        raise RuntimeError("nvcc failed linking libsxhmm.so")
     return OUT
 
 

@@ -11,6 +11,7 @@
 // clustering of multi-domain regions and the final bit scores.  Every f32/f64
 // operation is in the reference's order, so results are bit-identical to it.
 #include <algorithm>
+#include <cassert>
 #include <cstring>
 #include <optional>
 
@@ -137,11 +138,25 @@ struct Sample {  // p7_spcoord_s
 // Full-matrix workspaces of envelope rescoring: one set per thread, reused by
 // every EnvelopeScorer the thread creates (a fresh set per pair faulted in
 // megabytes of new pages every time).  Each use re-initialises what it reads,
-// and a thread runs one scorer at a time.
+// and a thread runs one scorer at a time; `in_use` checks that last point
+// (a scorer constructed while another one of the same thread is alive would
+// share, and overwrite, its matrices).
 struct ScorerWork {
   Mat fx, bx;
   Post pp;
   std::vector<float> om, oi, od;
+  bool in_use = false;
+};
+// Claims the thread's workspace for the lifetime of one EnvelopeScorer.
+struct WorkClaim {
+  ScorerWork& w;
+  explicit WorkClaim(ScorerWork& ws) : w(ws) {
+    assert(!w.in_use && "two EnvelopeScorer objects alive on one thread");
+    w.in_use = true;
+  }
+  ~WorkClaim() { w.in_use = false; }
+  WorkClaim(const WorkClaim&) = delete;
+  WorkClaim& operator=(const WorkClaim&) = delete;
 };
 ScorerWork& scorer_work() {
   thread_local ScorerWork w;
@@ -878,6 +893,7 @@ class EnvelopeScorer {
   const SearchOpts& o_;
   const size_t w_;
   ScorerWork& ws_ = scorer_work();
+  WorkClaim claim_{ws_};
   Mat& fx_ = ws_.fx;
   Mat& bx_ = ws_.bx;
   Post& pp_ = ws_.pp;

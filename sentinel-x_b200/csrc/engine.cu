@@ -38,10 +38,8 @@
 
 #include "../../include/sxhmm.h"
 #include "internal.hpp"
-#include "kernels.cuh"
-#include "adjoint.cuh"
+#include "shapes.hpp"
 #include "long.cuh"
-#include "envelope.cuh"
 #include "tuned_shapes.inc"
 
 using namespace sx;
@@ -136,144 +134,16 @@ struct PinnedBuf {
   }
 };
 
-// ---- kernel shapes ---------------------------------------------------------
-// MSV (G lanes per target, C columns per lane) shapes compiled into the library.
-struct MsvShape {
-  int g, c;
-};
-constexpr MsvShape kMsvShapes[] = {
-    {1, 8}, {1, 16}, {1, 24}, {1, 32}, {1, 40}, {1, 48}, {1, 56}, {1, 64},
-    {2, 8}, {2, 16}, {2, 24}, {2, 32}, {2, 40}, {2, 48}, {2, 56}, {2, 64},
-    {4, 8}, {4, 16}, {4, 24}, {4, 32}, {4, 40}, {4, 48}, {4, 56}, {4, 64},
-    {8, 8}, {8, 16}, {8, 24}, {8, 32}, {8, 40}, {8, 48}, {8, 56}, {8, 64},
-    {16, 8}, {16, 16}, {16, 24}, {16, 32}, {16, 40}, {16, 48}, {16, 56}, {16, 64},
-    {32, 8}, {32, 16}, {32, 24}, {32, 32}, {32, 40}, {32, 48}, {32, 56}, {32, 64},
-    // intermediate widths for the common range of M: half the column padding
-    {2, 36}, {2, 44}, {2, 52}, {2, 60}, {4, 36}, {4, 44}, {4, 52}, {4, 60},
-    {8, 36}, {8, 44}, {8, 52}, {8, 60}};
-constexpr int kNumMsvShapes = sizeof(kMsvShapes) / sizeof(kMsvShapes[0]);
-constexpr int kMaxM = 2048;  // columns of the warp-chunked and lane-group kernels
-// Longer profiles (marker models of long proteins) run through the long kernels.
-inline bool is_long(int m) { return m > kMaxM; }
-// Viterbi lane-group shapes (G lanes per pair, C columns per lane).
-// Viterbi lane-group shapes: G lanes per pair, C columns per lane, rt = the
-// transition rows held in registers for the whole pair (C <= 16).
-struct VitShape {
-  int g, c, rt;
-};
-constexpr VitShape kVitShapes[] = {{1, 8, 0},   {2, 8, 0},   {4, 8, 0},   {8, 8, 0},   {16, 8, 0},  {32, 8, 0},
-                                   {1, 16, 0},  {2, 16, 0},  {4, 16, 0},  {8, 16, 0},  {16, 16, 0}, {32, 16, 0},
-                                   {4, 24, 0},  {8, 24, 0},  {16, 24, 0}, {32, 24, 0}, {32, 32, 0}, {32, 48, 0},
-                                   {32, 64, 0}, {4, 8, 1},   {8, 8, 1},   {16, 8, 1},  {32, 8, 1},  {32, 16, 1}};
-// CTAs of one shape resident per SM: registers are capped at 128 for C <= 16
-// (two 256-thread CTAs) except with 16 register-held transition columns.
-constexpr int vit_ctas_per_sm(const VitShape& v) { return (v.c <= 16 && !(v.rt && v.c > 8)) ? 2 : 1; }
-constexpr int kNumVitShapes = sizeof(kVitShapes) / sizeof(kVitShapes[0]);
-constexpr int kMaxBins = 32;  // survivor lists per stage (vbins or Viterbi shapes)
-static_assert(kNumVitShapes <= kMaxBins, "too many Viterbi shapes");
-
-// Warp-chunked column counts (columns per lane, 32 lanes per pair).
-constexpr int kVcBins[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64};
-constexpr int kNumVbins = sizeof(kVcBins) / sizeof(kVcBins[0]);
-
-typedef void (*MsvFn)(const MsvTile*, const DevProfile*, const Thresholds*, const float4*, const uint8_t*,
-                      const int64_t*, const int32_t*, const float4*, const int32_t*, float*, const int32_t*, PairRec*,
-                      const BinRegion*, unsigned*, unsigned*);
-typedef void (*VitFn)(const PairRec*, const unsigned*, const BinRegion*, int, PairRec*, const BinRegion*, unsigned*,
-                      unsigned*, const DevProfile*, const Thresholds*, const float*, const uint8_t*, const int64_t*,
-                      const int32_t*, const float4*, float, float*);
-typedef void (*VitGFn)(const PairRec*, const unsigned*, const BinRegion*, int, PairRec*, const BinRegion*, unsigned*,
-                       unsigned*, const DevProfile*, const Thresholds*, const float4*, const uint8_t*, const int64_t*,
-                       const int32_t*, const float4*, float, float*, unsigned*);
-typedef void (*FwdFn)(const PairRec*, const unsigned*, const BinRegion*, int, PairRec*, const BinRegion*, unsigned*,
-                      unsigned*, const DevProfile*, const Thresholds*, const float*, const uint8_t*, const int64_t*,
-                      const int32_t*, const float4*, float, float*, const int64_t*);
-typedef void (*BwdFn)(const PairRec*, const unsigned*, const BinRegion*, int, const DevProfile*, const float*,
-                      const uint8_t*, const int64_t*, const int32_t*, const float4*, float*, const int64_t*);
-typedef void (*AdjFFn)(const sxk::AdjPair*, int, const DevProfile*, const float*, const uint8_t*, const int64_t*,
-                       const int32_t*, const float4*, float*, double*, double*);
-typedef void (*AdjBFn)(const sxk::AdjPair*, int, const DevProfile*, const float*, const uint8_t*, const int64_t*,
-                       const int32_t*, const float4*, float*, const double*, const double*, float*);
-
-template <int I>
-struct MsvTable {
-  static void fill(MsvFn* t) {
-    t[I] = sxk::msv_kernel<kMsvShapes[I].g, kMsvShapes[I].c>;
-    MsvTable<I + 1>::fill(t);
-  }
-};
-template <>
-struct MsvTable<kNumMsvShapes> {
-  static void fill(MsvFn*) {}
-};
-template <int I>
-struct VitGTable {
-  static void fill(VitGFn* t) {
-    t[I] = sxk::viterbi_g_kernel<kVitShapes[I].g, kVitShapes[I].c, kVitShapes[I].rt != 0>;
-    VitGTable<I + 1>::fill(t);
-  }
-};
-template <>
-struct VitGTable<kNumVitShapes> {
-  static void fill(VitGFn*) {}
-};
-template <int I>
-struct VbinTable {
-  static void fill(VitFn* v, FwdFn* f, FwdFn* fs, BwdFn* b, AdjFFn* af, AdjBFn* ab) {
-    v[I] = sxk::viterbi_kernel<kVcBins[I]>;
-    f[I] = sxk::forward_kernel<kVcBins[I]>;
-    fs[I] = sxk::forward_kernel<kVcBins[I], true>;
-    b[I] = sxk::backward_kernel<kVcBins[I]>;
-    af[I] = sxk::adjoint_forward_kernel<kVcBins[I]>;
-    ab[I] = sxk::adjoint_backward_kernel<kVcBins[I]>;
-    VbinTable<I + 1>::fill(v, f, fs, b, af, ab);
-  }
-};
-template <>
-struct VbinTable<kNumVbins> {
-  static void fill(VitFn*, FwdFn*, FwdFn*, BwdFn*, AdjFFn*, AdjBFn*) {}
-};
-
-typedef void (*EnvPassFn)(const sxk::EnvRec*, int, const DevProfile*, const float*, const uint8_t*, const int64_t*,
-                          float*, float*);
-typedef void (*EnvPostFn)(const sxk::EnvRec*, int, const DevProfile*, const float*, float*, float*, const double*,
-                          float*);
-template <int I>
-struct EnvTable {
-  static void fill(EnvPassFn* f, EnvPassFn* b, EnvPostFn* p, EnvPassFn* rf) {
-    f[I] = sxk::env_forward_kernel<kVcBins[I]>;
-    b[I] = sxk::env_backward_kernel<kVcBins[I]>;
-    p[I] = sxk::env_post_kernel<kVcBins[I]>;
-    rf[I] = sxk::env_forward_kernel<kVcBins[I], true>;
-    EnvTable<I + 1>::fill(f, b, p, rf);
-  }
-};
-template <>
-struct EnvTable<kNumVbins> {
-  static void fill(EnvPassFn*, EnvPassFn*, EnvPostFn*, EnvPassFn*) {}
-};
-
-struct KernelTables {
-  MsvFn msv[kNumMsvShapes];
-  EnvPassFn envf[kNumVbins], envb[kNumVbins];
-  EnvPostFn envp[kNumVbins];
-  EnvPassFn regf[kNumVbins];
-  VitFn vit[kNumVbins];
-  FwdFn fwd[kNumVbins];
-  FwdFn fwd_scan[kNumVbins];  // the F3 pre-screen
-  BwdFn bwd[kNumVbins];
-  AdjFFn adjf[kNumVbins];
-  AdjBFn adjb[kNumVbins];
-  VitGFn vitg[kNumVitShapes];
-  KernelTables() {
-    MsvTable<0>::fill(msv);
-    VitGTable<0>::fill(vitg);
-    VbinTable<0>::fill(vit, fwd, fwd_scan, bwd, adjf, adjb);
-    EnvTable<0>::fill(envf, envb, envp, regf);
-  }
-};
 const KernelTables& kernels() {
-  static KernelTables t;
+  static const KernelTables t = [] {
+    KernelTables k;
+    fill_msv_tables(k);
+    fill_msv16_tables(k);
+    fill_vit_tables(k);
+    fill_vbin_tables(k);
+    fill_env_tables(k);
+    return k;
+  }();
   return t;
 }
 
@@ -515,6 +385,10 @@ struct Slot {
   DevBuf<unsigned> cursor;  // kMaxBins pair cursors of the Viterbi launches
   DevBuf<double> cells;     // DP cells entering each stage (stats)
   DevBuf<MsvTile> tiles;
+  DevBuf<sxk::PackedTile> ptiles;  // packed pre-screen tiles
+  DevBuf<int32_t> rlist;           // pre-screen survivors: target indices, rcap per profile of the block
+  DevBuf<unsigned> rcount;         // survivors per profile of the block
+  cudaEvent_t pre_done = nullptr;  // pre-screen finished (its time, for the stats)
   void create() {
     int least = 0, greatest = 0;
     CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -525,6 +399,7 @@ struct Slot {
     hi.create(greatest, 8);
     lo.create(least, 5);
     for (auto& e : ev) CK(cudaEventCreate(&e));
+    CK(cudaEventCreate(&pre_done));
     CK(cudaEventCreateWithFlags(&msv_done, cudaEventDisableTiming));
   }
   void destroy() {
@@ -533,6 +408,7 @@ struct Slot {
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (msv_done) cudaEventDestroy(msv_done);
+    if (pre_done) cudaEventDestroy(pre_done);
   }
 };
 
@@ -565,6 +441,13 @@ struct sx_engine {
   // [0] MSV, [1] Viterbi; empty or -1 = the built-in choice
   std::vector<int16_t> shape_table[2];
   int64_t mem_free = 0;     // device memory free when the engine was created
+  // Lifetime: profile and target sets point at their engine.  sx_destroy
+  // releases the engine's streams at once, but the engine object itself lives
+  // until the last of its sets is freed, so a set freed after its engine (a
+  // garbage-collected binding, say) never touches freed memory.
+  std::mutex life_mu;
+  int64_t live_sets = 0;
+  bool destroyed = false;
   BlockPool target_blocks;  // device memory of freed target sets
   HostBytePool target_bytes;  // host residue buffers of freed target sets
   // envelope passes of the host domain definition (used by the host pool's
@@ -600,6 +483,7 @@ struct sx_profiles {
   DevBuf<sxk::PlainProfile> d_pprof;  // plain one-pair-per-block layout
   DevBuf<float> d_plain;
   DevBuf<float4> d_msv;
+  DevBuf<uint2> d_qimg;  // quantized MSV images of the pre-screen (int16, 4 columns per uint2)
   DevBuf<float4> d_vit;  // Viterbi lane-group images
   DevBuf<float> d_vfb;
   DevBuf<double> d_bias;
@@ -766,6 +650,37 @@ void pack_images(const ProfileHost& h, const DevProfile& d, float4* msv, float4*
   }
 }
 
+// Quantized MSV image of the packed pre-screen (prescreen.cuh): the match
+// scores in units of 2^-9 nat rounded up after adding 2^-12 nat, clamped up to
+// -16 nats (-inf included), -32 nats past column M, in the lane-major chunk
+// layout of the profile's f32 MSV image (4 columns per uint2).  Returns the
+// largest rounded score of a real column; the profile's cap is 32767 minus it.
+int pack_qimage(const ProfileHost& h, const DevProfile& d, uint2* out) {
+  const int m = h.m, G = d.msv_g, C = d.msv_c, NC4 = C / 4;
+  int emax = sxk::kQ16EFloor;
+  auto q = [&](int x, int k) -> int {
+    if (k > m) return sxk::kQ16EPad;
+    const float e = h.msc_row(x)[k];
+    if (!(e > -1e30f)) return sxk::kQ16EFloor;  // -inf (and NaN, which no configured profile has)
+    const double u = std::ceil(((double)e + std::ldexp(1.0, -12)) * 512.0);
+    const int v = (int)std::max<double>(u, (double)sxk::kQ16EFloor);
+    emax = std::max(emax, v);
+    return v;
+  };
+  uint2* base = out + d.q_off;
+  for (int x = 0; x < 25; x++)
+    for (int j = 0; j < G; j++)
+      for (int c4 = 0; c4 < NC4; c4++) {
+        int v[4];
+        for (int e = 0; e < 4; e++) v[e] = q(x, j * C + c4 * 4 + e + 1);
+        uint2 w;
+        w.x = (uint32_t)(v[0] & 0xffff) | ((uint32_t)(v[1] & 0xffff) << 16);
+        w.y = (uint32_t)(v[2] & 0xffff) | ((uint32_t)(v[3] & 0xffff) << 16);
+        base[((size_t)x * NC4 + c4) * G + j] = w;
+      }
+  return emax;
+}
+
 // Composition-bias filter table (src/hmmer/pipeline.rs:110-131): 54 doubles.
 void pack_bias(const ProfileHost& h, double* b) {
   const int m = h.m;
@@ -793,7 +708,7 @@ void pack_profiles(sx_profiles* P) {
   const size_t np = P->h.size();
   P->dp.resize(np);
   P->msv_shape.resize(np);
-  int64_t msv_total = 0, vfb_total = 0, vit_total = 0;
+  int64_t msv_total = 0, vfb_total = 0, vit_total = 0, q_total = 0;
   for (size_t i = 0; i < np; i++) {
     const ProfileHost& h = P->h[i];
     DevProfile& d = P->dp[i];
@@ -806,6 +721,7 @@ void pack_profiles(sx_profiles* P) {
       d.msv_off = msv_total;
       d.vfb_off = vfb_total;
       d.vit_off = vit_total;
+      d.q_off = -1;
       continue;
     }
     const int s = shape_for(P->eng, 0, h.m);
@@ -818,6 +734,9 @@ void pack_profiles(sx_profiles* P) {
     d.vc = kVcBins[vb];
     d.msv_off = msv_total;
     msv_total += 25LL * (d.msv_c / 4) * d.msv_g;
+    d.q_off = q_total;
+    q_total += 25LL * (d.msv_c / 4) * d.msv_g;
+    d.q_tbm = (int32_t)std::ceil(((double)h.msv_tbm + std::ldexp(1.0, -17)) * 1048576.0);
     d.vfb_off = vfb_total;
     vfb_total += (int64_t)sxk::kImgRows * 32 * d.vc;
     d.vshape = shape_for(P->eng, 1, h.m);
@@ -829,8 +748,16 @@ void pack_profiles(sx_profiles* P) {
   std::vector<float4> vit((size_t)std::max<int64_t>(vit_total, 1));
   std::vector<float> vfb((size_t)vfb_total);
   std::vector<double> bias(np * 54);
+  std::vector<uint2> qimg((size_t)std::max<int64_t>(q_total, 1));
   for (size_t i = 0; i < np; i++) {
-    if (P->dp[i].vbin >= 0) pack_images(P->h[i], P->dp[i], msv.data(), vit.data(), vfb.data());
+    if (P->dp[i].vbin >= 0) {
+      pack_images(P->h[i], P->dp[i], msv.data(), vit.data(), vfb.data());
+      // a profile whose rounded scores leave less than half of the int16
+      // range as headroom (scores above +16 nats) stays on the exact kernel
+      const int emax = pack_qimage(P->h[i], P->dp[i], qimg.data());
+      if (emax < 8192) P->dp[i].q_cap = 32767 - emax;
+      else P->dp[i].q_off = -1;
+    }
     pack_bias(P->h[i], bias.data() + i * 54);
   }
   // plain layout: 25 msc rows then mm mi md im ii dm dd bm, each M+1 long;
@@ -862,6 +789,7 @@ void pack_profiles(sx_profiles* P) {
   P->d_plain.upload(plain.data(), plain.size(), s);
   P->d_prof.upload(P->dp.data(), np, s);
   P->d_msv.upload(msv.data(), msv.size(), s);
+  P->d_qimg.upload(qimg.data(), qimg.size(), s);
   P->d_vit.upload(vit.data(), vit.size(), s);
   P->d_vfb.upload(vfb.data(), vfb.size(), s);
   P->d_bias.upload(bias.data(), bias.size(), s);
@@ -1273,9 +1201,18 @@ std::vector<std::vector<MsvTile>> make_all_pairs_tiles(const sx_engine* E, const
   return by_shape;
 }
 
+// Shared memory of an MSV-shaped CTA (f32 image or interleaved packed image:
+// both 16 bytes per chunk of 4 columns), one shifted copy per quarter-warp group.
+size_t msv_smem(int s) {
+  const int g = kMsvShapes[s].g, c = kMsvShapes[s].c;
+  const int ncopy = g < 8 ? 8 / g : 1;
+  const size_t rowp = ((size_t)(c / 4) * g + 7) & ~(size_t)7;
+  return (size_t)ncopy * (25 * rowp + 8 + g) * sizeof(float4);
+}
+
 void launch_msv(sx_engine* E, Slot& S, Streams& X, const sx_profiles* P, const sx_targets* T, const std::vector<std::vector<MsvTile>>& tiles,
                 const int32_t* d_list, float* d_scores, const int32_t* d_slot, PairRec* surv, const BinRegion* bins,
-                unsigned* counts) {
+                unsigned* counts, const unsigned* rcount = nullptr, unsigned rcap = 0, int p0 = 0) {
   const auto& K = kernels();
   std::vector<MsvTile> all;
   std::vector<size_t> start(kNumMsvShapes + 1, 0);
@@ -1298,18 +1235,99 @@ void launch_msv(sx_engine* E, Slot& S, Streams& X, const sx_profiles* P, const s
   int lane = 0;
   for (int s : order) {
     const size_t nt = start[s + 1] - start[s];
-    const int g = kMsvShapes[s].g, c = kMsvShapes[s].c;
-    const int ncopy = g < 8 ? 8 / g : 1;
-    const size_t rowp = ((size_t)(c / 4) * g + 7) & ~(size_t)7;
-    const size_t smem = (size_t)ncopy * (25 * rowp + 8 + g) * sizeof(float4);
+    const size_t smem = msv_smem(s);
     CK(cudaFuncSetAttribute((const void*)K.msv[s], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     K.msv[s]<<<(unsigned)nt, 256, smem, X.aux[lane++ % X.naux]>>>(
         S.tiles.p + start[s], P->d_prof.p, E->thr.p, P->d_msv.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_tpar.p,
-        d_list, d_scores, d_slot, surv, bins, counts, S.overflow.p);
+        d_list, d_scores, d_slot, surv, bins, counts, S.overflow.p, rcount, rcap, p0);
     E->stats.kernel_launches++;
   }
   CK(cudaGetLastError());
   join_aux(X);
+}
+
+// The block's pre-screened profiles: pairs of one MSV shape (similar M
+// adjacent) as tiles over slices of the length-sorted targets, grouped by shape.
+std::vector<std::vector<sxk::PackedTile>> make_packed_tiles(const sx_engine* E, const sx_profiles* P,
+                                                            const sx_targets* T, const std::vector<int>& prof) {
+  std::vector<std::vector<sxk::PackedTile>> by_shape(kNumMsvShapes);
+  const int nt = (int)T->len.size();
+  if (nt == 0 || prof.empty()) return by_shape;
+  std::vector<std::vector<int>> group(kNumMsvShapes);
+  for (int pi : prof) group[P->msv_shape[pi]].push_back(pi);
+  std::vector<std::pair<int, int>> pairs;  // (pa, pb), pb = -1 for the odd one
+  for (auto& g : group) {
+    std::stable_sort(g.begin(), g.end(), [&](int a, int b) { return P->h[a].m > P->h[b].m; });
+    for (size_t q = 0; q < g.size(); q += 2) pairs.emplace_back(g[q], q + 1 < g.size() ? g[q + 1] : -1);
+  }
+  const int np = (int)pairs.size();
+  int nslices = (int)std::ceil(16.0 * E->num_sms * 2 / std::max(1, np));
+  nslices = std::max(1, std::min(nslices, std::max(1, nt / 32)));
+  std::vector<int> cut(nslices + 1, nt);
+  cut[0] = 0;
+  {
+    double acc = 0, per = T->residues / nslices;
+    int s = 1;
+    for (int q = 0; q < nt && s < nslices; q++) {
+      acc += T->len[T->order[q]];
+      if (acc >= per * s) cut[s++] = q + 1;
+    }
+  }
+  for (const auto& pr : pairs)
+    for (int s = 0; s < nslices; s++)
+      if (cut[s + 1] > cut[s]) by_shape[P->msv_shape[pr.first]].push_back({pr.first, pr.second, cut[s], cut[s + 1]});
+  return by_shape;
+}
+
+// Packed pre-screen of a block (profiles `prof`, all with a quantized image):
+// the pairs whose bound passes F1 land in the per-profile rescoring lists of
+// slot S (region (p - p0) * rcap of S.rlist, counts in S.rcount).
+void launch_prescreen(sx_engine* E, Slot& S, Streams& X, const sx_profiles* P, const sx_targets* T,
+                      const std::vector<int>& prof, unsigned rcap, int p0) {
+  const auto& K = kernels();
+  auto tiles = make_packed_tiles(E, P, T, prof);
+  std::vector<sxk::PackedTile> all;
+  std::vector<size_t> start(kNumMsvShapes + 1, 0);
+  for (int s = 0; s < kNumMsvShapes; s++) {
+    start[s] = all.size();
+    all.insert(all.end(), tiles[s].begin(), tiles[s].end());
+  }
+  start[kNumMsvShapes] = all.size();
+  if (all.empty()) return;
+  S.ptiles.upload(all.data(), all.size(), X.main);
+  std::vector<int> order;
+  std::vector<double> work(kNumMsvShapes, 0.0);
+  for (int s = 0; s < kNumMsvShapes; s++)
+    if (start[s + 1] > start[s]) {
+      order.push_back(s);
+      for (size_t q = start[s]; q < start[s + 1]; q++) work[s] += (double)all[q].end - all[q].begin;
+    }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+  fork_aux(X);
+  int lane = 0;
+  for (int s : order) {
+    const size_t smem = msv_smem(s);
+    CK(cudaFuncSetAttribute((const void*)K.msv16[s], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    K.msv16[s]<<<(unsigned)(start[s + 1] - start[s]), 256, smem, X.aux[lane++ % X.naux]>>>(
+        S.ptiles.p + start[s], P->d_prof.p, E->thr.p, P->d_qimg.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_tpar.p,
+        T->d_order.p, S.rlist.p, rcap, S.rcount.p, p0, S.overflow.p, nullptr, nullptr, 0);
+    E->stats.kernel_launches++;
+  }
+  CK(cudaGetLastError());
+  join_aux(X);
+}
+
+// Exact MSV of the pre-screen's survivors: per profile `nsub` strided
+// sub-tiles over its rescoring list; scores and F1 decisions as in a full
+// MSV pass (survivors appended to the stage-0 lists).
+void launch_rescore(sx_engine* E, Slot& S, Streams& X, const sx_profiles* P, const sx_targets* T,
+                    const std::vector<int>& prof, unsigned rcap, int p0) {
+  std::vector<std::vector<MsvTile>> tiles(kNumMsvShapes);
+  const int nsub = std::max(2, std::min(32, (int)std::ceil(4.0 * E->num_sms / std::max<size_t>(1, prof.size()))));
+  for (int pi : prof)
+    for (int q = 0; q < nsub; q++) tiles[P->msv_shape[pi]].push_back({pi, q, nsub, 0});
+  launch_msv(E, S, X, P, T, tiles, S.rlist.p, nullptr, nullptr, S.lists[0].p, S.bins[0].p, S.counts.p, S.rcount.p,
+             rcap, p0);
 }
 
 // One filter stage over per-vbin lists: stage `si` reads lists[si] and writes lists[si+1].
@@ -1802,6 +1820,8 @@ std::vector<std::pair<int, int>> profile_blocks(const sx_engine* E, const sx_pro
 struct BlockRun {
   int p0 = 0, p1 = 0;
   int attempt = 0;  // survivor-list sizing attempt; lists grow 4x per overflow
+  std::vector<int> screened;  // profiles that go through the packed pre-screen
+  unsigned rcap = 0;          // rescoring-list capacity per profile
   StageLists L[4];
   std::vector<double> pairs_in_bin, pairs_in_vs;
   double cells_total = 0;
@@ -1860,10 +1880,32 @@ void cascade_launch(sx_engine* E, Slot& S, const sx_profiles* P, const sx_target
     }
     CK(cudaGetLastError());
   } else {
+    // Profiles with a quantized image go through the packed pre-screen, then
+    // the exact MSV of its survivors; the others straight through the exact
+    // kernel.  Either way the stage-0 lists receive exactly the pairs whose
+    // f32 MSV score passes F1.
+    R.screened.clear();
+    if (!(E->flags & SX_FLAG_NO_PRESCREEN) && nt > 0)
+      for (int pi = R.p0; pi < R.p1; pi++)
+        if (th[pi].exact && P->dp[pi].q_off >= 0) R.screened.push_back(pi);
+    R.rcap = (unsigned)(full ? nt : std::min<double>((double)nt, scale * (0.05 * (double)nt + 1024)));
+    if ((int64_t)(R.p1 - R.p0) * (int64_t)R.rcap >= (int64_t)INT32_MAX) R.screened.clear();
+    std::vector<char> scr(R.p1 - R.p0, 0);
+    for (int pi : R.screened) scr[pi - R.p0] = 1;
     auto tiles = make_all_pairs_tiles(E, P, T, R.p0, R.p1);
     for (auto& v : tiles)
-      v.erase(std::remove_if(v.begin(), v.end(), [&](const MsvTile& t) { return !th[t.p].exact; }), v.end());
+      v.erase(std::remove_if(v.begin(), v.end(),
+                             [&](const MsvTile& t) { return !th[t.p].exact || scr[t.p - R.p0]; }),
+              v.end());
     launch_msv(E, S, S.lo, P, T, tiles, T->d_order.p, nullptr, nullptr, S.lists[0].p, S.bins[0].p, S.counts.p);
+    if (!R.screened.empty()) {
+      S.rlist.alloc((size_t)(R.p1 - R.p0) * R.rcap);
+      S.rcount.alloc((size_t)(R.p1 - R.p0));
+      CK(cudaMemsetAsync(S.rcount.p, 0, sizeof(unsigned) * (R.p1 - R.p0), s));
+      launch_prescreen(E, S, S.lo, P, T, R.screened, R.rcap, R.p0);
+      CK(cudaEventRecord(S.pre_done, s));
+      launch_rescore(E, S, S.lo, P, T, R.screened, R.rcap, R.p0);
+    }
   }
   CK(cudaEventRecord(S.ev[1], s));
   CK(cudaEventRecord(S.msv_done, s));
@@ -1924,6 +1966,20 @@ bool cascade_finish(sx_engine* E, Slot& S, const sx_profiles* P, const sx_target
   E->stats.cells[2] += scells[1];
   E->stats.cells[3] += scells[2];
   E->stats.ms[0] += elapsed_ms(S.ev[0], S.ev[1]);
+  if (!R.screened.empty()) {
+    std::vector<unsigned> rc((size_t)(R.p1 - R.p0));
+    CK(cudaMemcpyAsync(rc.data(), S.rcount.p, sizeof(unsigned) * rc.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    double cells = 0;
+    for (int pi : R.screened) {
+      E->stats.prescreen_pairs_out += std::min(rc[pi - R.p0], R.rcap);
+      cells += (double)P->h[pi].m;
+    }
+    E->stats.prescreen_pairs_in += (int64_t)R.screened.size() * (int64_t)T->len.size();
+    E->stats.prescreen_cells += cells * T->residues;
+    E->stats.prescreen_ms += elapsed_ms(S.ev[0], S.pre_done);
+    E->stats.rescore_ms += elapsed_ms(S.pre_done, S.ev[1]);
+  }
   E->stats.ms[1] += elapsed_ms(S.ev[2], S.ev[3]);
   E->stats.ms[2] += elapsed_ms(S.ev[3], S.ev[4]);
   E->stats.ms[3] += elapsed_ms(S.ev[4], S.ev[5]);
@@ -2343,7 +2399,29 @@ void sx_destroy(sx_engine* e) {
       cudaStreamDestroy(st);
     }
   if (e->env_ev) cudaEventDestroy(e->env_ev);
-  delete e;
+  e->env_stream = e->env_stream2 = nullptr;
+  e->env_ev = nullptr;
+  bool last;
+  {
+    std::lock_guard<std::mutex> g(e->life_mu);
+    e->destroyed = true;
+    last = e->live_sets == 0;
+  }
+  if (last) delete e;
+}
+
+// A set handed to the caller keeps its engine object alive (see sx_engine).
+static void engine_ref(sx_engine* e) {
+  std::lock_guard<std::mutex> g(e->life_mu);
+  e->live_sets++;
+}
+static void engine_unref(sx_engine* e) {
+  bool last;
+  {
+    std::lock_guard<std::mutex> g(e->life_mu);
+    last = --e->live_sets == 0 && e->destroyed;
+  }
+  if (last) delete e;
 }
 
 static int finish_profiles(sx_engine* e, std::unique_ptr<sx_profiles> p, sx_profiles** out) {
@@ -2353,6 +2431,7 @@ static int finish_profiles(sx_engine* e, std::unique_ptr<sx_profiles> p, sx_prof
   } catch (const CudaError& ce) {
     return fail(ce.code, ce.msg);
   }
+  engine_ref(e);
   *out = p.release();
   return SX_OK;
 }
@@ -2470,8 +2549,10 @@ int sx_profiles_info(const sx_profiles* p, int32_t i, sx_profile_info* out) {
 
 void sx_profiles_free(sx_profiles* p) {
   if (!p) return;
-  cudaSetDevice(p->eng->device);
+  sx_engine* e = p->eng;
+  cudaSetDevice(e->device);
   delete p;
+  engine_unref(e);
 }
 
 static int finish_targets(sx_engine* e, std::unique_ptr<sx_targets> t, sx_targets** out) {
@@ -2482,6 +2563,7 @@ static int finish_targets(sx_engine* e, std::unique_ptr<sx_targets> t, sx_target
   } catch (const CudaError& ce) {
     return fail(ce.code, ce.msg);
   }
+  engine_ref(e);
   *out = t.release();
   return SX_OK;
 }
@@ -2544,8 +2626,10 @@ int64_t sx_targets_count(const sx_targets* t) { return t ? (int64_t)t->len.size(
 
 void sx_targets_free(sx_targets* t) {
   if (!t) return;
-  cudaSetDevice(t->eng->device);
+  sx_engine* e = t->eng;
+  cudaSetDevice(e->device);
   delete t;
+  engine_unref(e);
 }
 
 int sx_search(sx_engine* e, const sx_profiles* p, const sx_targets* t, const sx_search_cfg* cfg, sx_hits** out) {
@@ -2820,6 +2904,129 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
       long_rows(e, p, t, lpairs, [&](size_t first, size_t n, const float* f, const float* b, const std::vector<int64_t>& off) {
         for (size_t q = 0; q < n; q++) put(lng[first + q], f + off[q], b + off[q]);
       });
+    }
+  } catch (const CudaError& ce) {
+    return fail(ce.code, ce.msg);
+  }
+  return SX_OK;
+}
+
+int sx_score_prescreens(sx_engine* e, const sx_profiles* p, const sx_targets* t, const int32_t* pair_profile,
+                        const int32_t* pair_target, size_t npairs, float* msv_bound, float* fwd_scan) {
+  if (!e || !p || !t || (npairs && (!pair_profile || !pair_target)))
+    return fail(SX_EINVAL, "sx_score_prescreens: NULL argument");
+  if (p->eng != e || t->eng != e) return fail(SX_EINVAL, "sx_score_prescreens: profiles/targets belong to another engine");
+  std::lock_guard<std::mutex> lk(e->mu);
+  const size_t np = p->h.size(), nt = t->len.size();
+  for (size_t i = 0; i < npairs; i++)
+    if (pair_profile[i] < 0 || (size_t)pair_profile[i] >= np || pair_target[i] < 0 || (size_t)pair_target[i] >= nt)
+      return fail(SX_EINVAL, "sx_score_prescreens: pair " + std::to_string(i) + " out of range");
+  if (npairs > (size_t)INT32_MAX) return fail(SX_EINVAL, "sx_score_prescreens: too many pairs");
+  for (size_t i = 0; i < npairs; i++) {
+    if (msv_bound) msv_bound[i] = NAN;
+    if (fwd_scan) fwd_scan[i] = NAN;
+  }
+  if (!npairs) return SX_OK;
+  try {
+    CK(cudaSetDevice(e->device));
+    cudaStream_t s = e->stream;
+    const auto& K = kernels();
+    std::vector<Thresholds> th(np, Thresholds{-INFINITY, -INFINITY, -INFINITY, 0});
+    e->thr.upload(th.data(), th.size(), s);
+    e->overflow.alloc(1);
+    CK(cudaMemsetAsync(e->overflow.p, 0, sizeof(unsigned), s));
+    if (msv_bound) {
+      // pairs of pre-screened profiles, sorted by (profile, length desc); one
+      // profile per tile (the high half is padding)
+      std::vector<int32_t> idx;
+      for (size_t i = 0; i < npairs; i++)
+        if (p->dp[pair_profile[i]].vbin >= 0 && p->dp[pair_profile[i]].q_off >= 0) idx.push_back((int32_t)i);
+      std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+        if (pair_profile[a] != pair_profile[b]) return pair_profile[a] < pair_profile[b];
+        return t->len[pair_target[a]] > t->len[pair_target[b]];
+      });
+      const size_t n = idx.size();
+      if (n) {
+        std::vector<int32_t> lst(n), slot(n);
+        for (size_t q = 0; q < n; q++) {
+          lst[q] = pair_target[idx[q]];
+          slot[q] = idx[q];
+        }
+        std::vector<std::vector<sxk::PackedTile>> tiles(kNumMsvShapes);
+        size_t q = 0;
+        while (q < n) {
+          size_t r = q;
+          const int pp = pair_profile[idx[q]];
+          while (r < n && pair_profile[idx[r]] == pp) r++;
+          for (size_t a = q; a < r; a += 4096)
+            tiles[p->msv_shape[pp]].push_back({pp, -1, (int32_t)a, (int32_t)std::min(r, a + 4096)});
+          q = r;
+        }
+        e->plist.upload(lst.data(), n, s);
+        e->slots.upload(slot.data(), n, s);
+        e->scores.alloc(npairs);
+        std::vector<float> nanv(npairs, NAN);
+        CK(cudaMemcpyAsync(e->scores.p, nanv.data(), sizeof(float) * npairs, cudaMemcpyHostToDevice, s));
+        Slot& S = e->sl[0];
+        for (int sh = 0; sh < kNumMsvShapes; sh++) {
+          if (tiles[sh].empty()) continue;
+          S.ptiles.upload(tiles[sh].data(), tiles[sh].size(), s);
+          const size_t smem = msv_smem(sh);
+          CK(cudaFuncSetAttribute((const void*)K.msv16[sh], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          K.msv16[sh]<<<(unsigned)tiles[sh].size(), 256, smem, s>>>(
+              S.ptiles.p, p->d_prof.p, e->thr.p, p->d_qimg.p, t->d_res.p, t->d_off.p, t->d_len.p, t->d_tpar.p,
+              e->plist.p, nullptr, 0, nullptr, 0, e->overflow.p, e->scores.p, e->slots.p, 0);
+          CK(cudaGetLastError());
+          CK(cudaStreamSynchronize(s));  // the tile buffer is reused by the next shape
+        }
+        CK(cudaMemcpyAsync(msv_bound, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+      }
+    }
+    if (fwd_scan) {
+      // every pair through the F3 pre-screen with a threshold of -inf: all of
+      // them come out of the kernel carrying its Forward estimate
+      std::vector<PairRec> recs;
+      std::vector<BinRegion> reg(kMaxBins);
+      std::vector<unsigned> cnt(kMaxBins, 0);
+      std::vector<std::vector<int32_t>> byb(kMaxBins);
+      for (size_t i = 0; i < npairs; i++)
+        if (p->dp[pair_profile[i]].vbin >= 0) byb[p->dp[pair_profile[i]].vbin].push_back((int32_t)i);
+      for (int b = 0; b < kMaxBins; b++) {
+        reg[b].off = (int64_t)recs.size();
+        reg[b].cap = (uint32_t)byb[b].size();
+        reg[b].pad = 0;
+        cnt[b] = (unsigned)byb[b].size();
+        for (int32_t i : byb[b]) recs.push_back({pair_profile[i], pair_target[i], 0.f, 0.f, 0.f, 0.f, i, 0});
+      }
+      if (!recs.empty()) {
+        Slot& S = e->sl[0];
+        S.lists[2].upload(recs.data(), recs.size(), s);
+        S.lists[3].alloc(recs.size());
+        S.bins[2].upload(reg.data(), reg.size(), s);
+        S.bins[3].upload(reg.data(), reg.size(), s);
+        e->counts.alloc(4 * kMaxBins);
+        CK(cudaMemcpyAsync(e->counts.p + 2 * kMaxBins, cnt.data(), sizeof(unsigned) * kMaxBins, cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(e->counts.p + 3 * kMaxBins, 0, sizeof(unsigned) * kMaxBins, s));
+        for (int b = 0; b < kNumVbins; b++) {
+          if (!cnt[b]) continue;
+          K.fwd_scan[b]<<<warp_ctas(e->num_sms, cnt[b]), 32, 0, s>>>(
+              S.lists[2].p, e->counts.p + 2 * kMaxBins, S.bins[2].p, b, S.lists[3].p, S.bins[3].p,
+              e->counts.p + 3 * kMaxBins, e->overflow.p, p->d_prof.p, e->thr.p, p->d_vfb.p, t->d_res.p, t->d_off.p,
+              t->d_len.p, t->d_xsc.p, kSlackBits, nullptr, nullptr);
+        }
+        CK(cudaGetLastError());
+        std::vector<PairRec> out(recs.size());
+        CK(cudaMemcpyAsync(out.data(), S.lists[3].p, sizeof(PairRec) * out.size(), cudaMemcpyDeviceToHost, s));
+        std::vector<unsigned> oc(kMaxBins);
+        CK(cudaMemcpyAsync(oc.data(), e->counts.p + 3 * kMaxBins, sizeof(unsigned) * kMaxBins, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (int b = 0; b < kNumVbins; b++)
+          for (unsigned q = 0; q < std::min(oc[b], cnt[b]); q++) {
+            const PairRec& r = out[reg[b].off + q];
+            fwd_scan[r.slot] = r.fwd;
+          }
+      }
     }
   } catch (const CudaError& ce) {
     return fail(ce.code, ce.msg);

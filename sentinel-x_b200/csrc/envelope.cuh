@@ -744,7 +744,7 @@ __device__ __forceinline__ int trace_choose(uint32_t& rng, float (&v)[N]) {
 // region that leaves the matrix, or whose samples overflow the pool or the
 // per-trace buffer, is flagged (status 1) for the host to redo.  Pool records
 // carry the region's index `first + w` within the caller's batch.
-__global__ void __launch_bounds__(128) env_trace_kernel(const TraceRec* __restrict__ recs, int n,
+static __global__ void __launch_bounds__(128) env_trace_kernel(const TraceRec* __restrict__ recs, int n,
                                                         const float* __restrict__ cols,
                                                         const uint8_t* __restrict__ res,
                                                         const int64_t* __restrict__ toff,

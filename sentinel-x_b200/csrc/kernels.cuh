@@ -20,18 +20,21 @@ constexpr float kLn2 = 0.693147182464599609375f;
 constexpr unsigned kFull = 0xffffffffu;
 
 // ---- device records ------------------------------------------------------
-struct DevProfile {  // 56 bytes
+struct DevProfile {  // 72 bytes
   int32_t m;
   int32_t vc;        // columns per lane in the warp-chunked layout (32 lanes)
   int32_t vbin;      // survivor-list bin of vc
   int32_t msv_g;     // MSV lanes per target
   int32_t msv_c;     // MSV columns per lane
-  int32_t pad0;
+  int32_t q_cap;     // packed pre-screen: row maxima above this (int16 units) pass at once
   int64_t msv_off;   // float4 offset of the MSV shared-memory image
   int64_t vfb_off;   // float offset of the warp-chunked image (kImgRows rows of 32*vc)
   float msv_tbm;
   int32_t vshape;    // Viterbi lane-group shape (index into the engine's shape table)
   int64_t vit_off;   // float4 offset of the Viterbi image (33 rows, lane-major for that shape)
+  int64_t q_off;     // uint2 offset of the quantized MSV image; -1: the profile is not pre-screened
+  int32_t q_tbm;     // msv_tbm rounded up, units of 2^-20 nat (pre-screen entry constant)
+  int32_t pad1;
 };
 struct Thresholds {  // per profile, per search: pass iff statistic >= threshold (bits)
   float s1, s2, s3;
@@ -131,7 +134,8 @@ __global__ void __launch_bounds__(256, 2) msv_kernel(const MsvTile* __restrict__
                                                   const float4* __restrict__ tpar, const int32_t* __restrict__ list,
                                                   float* __restrict__ score_out, const int32_t* __restrict__ slot,
                                                   PairRec* __restrict__ surv, const BinRegion* __restrict__ bins,
-                                                  unsigned* __restrict__ counts, unsigned* __restrict__ overflow) {
+                                                  unsigned* __restrict__ counts, unsigned* __restrict__ overflow,
+                                                  const unsigned* __restrict__ rcount, unsigned rcap, int p0) {
   static_assert(C % 4 == 0 && (G & (G - 1)) == 0 && G <= 32, "bad MSV shape");
   constexpr int NC4 = C / 4;
   constexpr int ROW4 = NC4 * G;  // float4 per residue row
@@ -155,7 +159,17 @@ __global__ void __launch_bounds__(256, 2) msv_kernel(const MsvTile* __restrict__
       for (int cp = 0; cp < NCOPY; cp++) sm_rows[cp * COPY4 + cp * G + x * ROWP + e] = v;
     }
   }
-  if (threadIdx.x == 0) s_next = tile.begin;
+  // Targets of the tile: list[first + k * stride] for first + k * stride < last.
+  // A rescoring tile (rcount != null) takes the pre-screen's survivors of its
+  // profile, region (p - p0) * rcap of the list, every `end`-th one from `begin`.
+  int first = tile.begin, last = tile.end, stride = 1;
+  if (rcount) {
+    const int q = tile.p - p0;
+    first = q * (int)rcap + tile.begin;
+    last = q * (int)rcap + (int)min(rcount[q], rcap);
+    stride = tile.end;
+  }
+  if (threadIdx.x == 0) s_next = 0;
   __syncthreads();
 
   const int lane = threadIdx.x & 31;
@@ -190,9 +204,9 @@ __global__ void __launch_bounds__(256, 2) msv_kernel(const MsvTile* __restrict__
         }
       }
       int e = 0;
-      if (j == 0) e = atomicAdd(&s_next, 1);
+      if (j == 0) e = first + atomicAdd(&s_next, 1) * stride;
       e = __shfl_sync(gmask, e, gl);
-      if (e < tile.end) {
+      if (e < last) {
         entry = e;
         tgt = list[e];
         L = tlen[tgt];
@@ -272,7 +286,7 @@ __global__ void __launch_bounds__(256, 2) msv_kernel(const MsvTile* __restrict__
 // the host re-checks survivors with the exact libm value.
 // btab per profile: eo0[25], eo1[25], t00, t01, t10, t11  (54 doubles)
 // ===========================================================================
-__global__ void __launch_bounds__(256) bias_kernel(const PairRec* __restrict__ in, const unsigned* __restrict__ in_counts,
+static __global__ void __launch_bounds__(256) bias_kernel(const PairRec* __restrict__ in, const unsigned* __restrict__ in_counts,
                                                    const BinRegion* __restrict__ in_bins, PairRec* __restrict__ out,
                                                    const BinRegion* __restrict__ out_bins, unsigned* __restrict__ out_counts,
                                                    unsigned* __restrict__ overflow, const double* __restrict__ btab,
@@ -320,7 +334,7 @@ __global__ void __launch_bounds__(256) bias_kernel(const PairRec* __restrict__ i
 // DP cells (sum of M * L) of the pairs in the per-bin lists (grid.y = bin):
 // the work a stage receives, for its GCUPS.  Double atomics per warp; the
 // order of the additions (and so the last bits) may vary between runs.
-__global__ void __launch_bounds__(256) stage_cells_kernel(const PairRec* __restrict__ lists,
+static __global__ void __launch_bounds__(256) stage_cells_kernel(const PairRec* __restrict__ lists,
                                                           const unsigned* __restrict__ counts,
                                                           const BinRegion* __restrict__ bins,
                                                           const DevProfile* __restrict__ profs,

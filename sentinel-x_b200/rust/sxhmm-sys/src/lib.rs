@@ -39,6 +39,7 @@ pub mod ffi {
     pub const SX_FLAG_ENV_HOST: u32 = 4;
     pub const SX_FLAG_TRACE_HOST: u32 = 8;
     pub const SX_FLAG_TRACE_DEVICE: u32 = 16;
+    pub const SX_FLAG_NO_PRESCREEN: u32 = 32;
 
     #[repr(C)]
     pub struct sx_engine {
@@ -162,6 +163,11 @@ pub mod ffi {
         pub cells: [f64; 8],
         pub ms: [f64; 8],
         pub kernel_launches: i64,
+        pub prescreen_pairs_in: i64,
+        pub prescreen_pairs_out: i64,
+        pub prescreen_cells: f64,
+        pub prescreen_ms: f64,
+        pub rescore_ms: f64,
     }
 
     extern "C" {
@@ -206,6 +212,9 @@ pub mod ffi {
         pub fn sx_score_pairs(e: *mut sx_engine, p: *const sx_profiles, t: *const sx_targets,
                               pair_profile: *const i32, pair_target: *const i32, npairs: usize, msv: *mut f32,
                               viterbi: *mut f32, forward: *mut f32, backward: *mut f32, bias: *mut f32) -> c_int;
+        pub fn sx_score_prescreens(e: *mut sx_engine, p: *const sx_profiles, t: *const sx_targets,
+                                   pair_profile: *const i32, pair_target: *const i32, npairs: usize,
+                                   msv_bound: *mut f32, fwd_scan: *mut f32) -> c_int;
         pub fn sx_posterior_grad(e: *mut sx_engine, p: *const sx_profiles, t: *const sx_targets,
                                  pair_profile: *const i32, pair_target: *const i32, npairs: usize, m: i32,
                                  d_msc: *mut f32, d_isc: *mut f32, d_trans: *mut f32, lnz: *mut f64) -> c_int;

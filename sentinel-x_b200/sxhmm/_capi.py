@@ -14,6 +14,7 @@ SX_FLAG_ENV_DEVICE = 2
 SX_FLAG_ENV_HOST = 4
 SX_FLAG_TRACE_HOST = 8
 SX_FLAG_TRACE_DEVICE = 16
+SX_FLAG_NO_PRESCREEN = 32
 
 # Every entry point declared in include/sxhmm.h, name -> (restype, argtypes).
 _P = C.c_void_p
@@ -60,7 +61,9 @@ class SxProfileArrays(C.Structure):
 
 class SxSearchStats(C.Structure):
     _fields_ = [("pairs_in", C.c_int64 * 8), ("pairs_out", C.c_int64 * 8), ("cells", C.c_double * 8),
-                ("ms", C.c_double * 8), ("kernel_launches", C.c_int64)]
+                ("ms", C.c_double * 8), ("kernel_launches", C.c_int64), ("prescreen_pairs_in", C.c_int64),
+                ("prescreen_pairs_out", C.c_int64), ("prescreen_cells", C.c_double), ("prescreen_ms", C.c_double),
+                ("rescore_ms", C.c_double)]
 
 
 _i32p = C.POINTER(C.c_int32)
@@ -102,6 +105,7 @@ SIGNATURES = {
     "sx_score_pairs": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, _fp, _fp, _fp, _fp, _fp]),
     "sx_posterior_grad": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, C.c_int32, _fp, _fp, _fp, _dp]),
     "sx_score_viterbi_static": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, _fp]),
+    "sx_score_prescreens": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, _fp, _fp]),
 }
 
 
@@ -154,10 +158,11 @@ class Engine:
     """One engine per device (sx_create)."""
 
     def __init__(self, device=0, host_threads=0, plain=False, batch_bytes=0, pipeline_blocks=0, envelopes="auto",
-                 traces="auto"):
+                 traces="auto", prescreen=True):
         lib = load_library()
         flags = (SX_FLAG_PLAIN if plain else 0) | {"auto": 0, "device": SX_FLAG_ENV_DEVICE,
                                                     "host": SX_FLAG_ENV_HOST}[envelopes]
+        flags |= 0 if prescreen else SX_FLAG_NO_PRESCREEN
         flags |= {"auto": 0, "device": SX_FLAG_TRACE_DEVICE, "host": SX_FLAG_TRACE_HOST}[traces]
         o = SxOpts(device, host_threads, flags, pipeline_blocks, batch_bytes)
         h = C.c_void_p()
@@ -241,7 +246,9 @@ class Engine:
         s = SxSearchStats()
         _check(_lib.sx_last_search_stats(self.h, C.byref(s)))
         return {"pairs_in": list(s.pairs_in), "pairs_out": list(s.pairs_out), "cells": list(s.cells),
-                "ms": list(s.ms), "kernel_launches": s.kernel_launches}
+                "ms": list(s.ms), "kernel_launches": s.kernel_launches,
+                "prescreen": {"pairs_in": s.prescreen_pairs_in, "pairs_out": s.prescreen_pairs_out,
+                              "cells": s.prescreen_cells, "ms": s.prescreen_ms, "rescore_ms": s.rescore_ms}}
 
     def score_pairs(self, profiles, targets, pp, pt, stages=("msv", "viterbi", "forward", "backward", "bias")):
         pp = np.ascontiguousarray(pp, dtype=np.int32)
@@ -254,6 +261,19 @@ class Engine:
         _check(_lib.sx_score_pairs(self.h, profiles.h, targets.h, _ptr(pp, C.c_int32), _ptr(pt, C.c_int32), n,
                                    p("msv"), p("viterbi"), p("forward"), p("backward"), p("bias")))
         return {s: v[:n] for s, v in out.items()}
+
+    def score_prescreens(self, profiles, targets, pp, pt):
+        """The two conservative screens for explicit pairs (sx_score_prescreens):
+        {"msv_bound": packed MSV pre-screen bound, "fwd_scan": F3 pre-screen
+        Forward score}, float32 arrays (nats)."""
+        pp = np.ascontiguousarray(pp, dtype=np.int32)
+        pt = np.ascontiguousarray(pt, dtype=np.int32)
+        n = len(pp)
+        mb = np.full(max(n, 1), np.nan, np.float32)
+        fs = np.full(max(n, 1), np.nan, np.float32)
+        _check(_lib.sx_score_prescreens(self.h, profiles.h, targets.h, _ptr(pp, C.c_int32), _ptr(pt, C.c_int32), n,
+                                        _ptr(mb, C.c_float), _ptr(fs, C.c_float)))
+        return {"msv_bound": mb[:n], "fwd_scan": fs[:n]}
 
     def posterior_grad(self, profiles, targets, pp, pt, m, out=None):
         """lnZ and its gradients for each pair (sx_posterior_grad).  `out`:

@@ -146,34 +146,57 @@ def background_seq(rng, n, freqs=None):
     return rng.choice(20, size=n, p=f).astype(np.uint8)
 
 
+def _cdf(p):
+    """The cumulative table numpy's Generator.choice(n, p=p) draws from."""
+    c = p.cumsum()
+    c /= c[-1]
+    return c
+
+
+def _walk_tables(p):
+    """Per-node cumulative tables of emit_homolog's draws (cached on p)."""
+    tab = getattr(p, "_walk", None)
+    if tab is None:
+        m = p.m
+        mat = [None] + [_cdf(p.mat[k]) for k in range(1, m + 1)]
+        ins = [_cdf(p.ins[k]) for k in range(m + 1)]
+        tm = [_cdf(p.t[k][0:3] / p.t[k][0:3].sum()) for k in range(m + 1)]
+        ti = [_cdf(p.t[k][3:5] / p.t[k][3:5].sum()) for k in range(m + 1)]
+        td = [_cdf(p.t[k][5:7] / p.t[k][5:7].sum()) for k in range(m + 1)]
+        tab = p._walk = (mat, ins, tm, ti, td)
+    return tab
+
+
 def emit_homolog(rng, p):
     """Digitised residues of one local path through p (entry in the first tenth
-    of the nodes, exit in the last tenth)."""
+    of the nodes, exit in the last tenth).  Every draw is the one
+    rng.choice(n, p=...) makes (one uniform, the first cumulative entry above
+    it), from tables computed once per profile."""
     m = p.m
     k = int(rng.integers(1, max(1, m // 10) + 1))
     kend = int(rng.integers(m - m // 10, m + 1)) if m >= 10 else m
     kend = max(kend, k)
+    mat, ins, tm, ti, td = _walk_tables(p)
     out = []
-    st = "M"
+    st = 0  # 0 M, 1 I, 2 D
     guard = 0
     while guard < 20 * m + 100:
         guard += 1
-        if st == "M":
-            out.append(rng.choice(20, p=p.mat[k]))
-        elif st == "I":
-            out.append(rng.choice(20, p=p.ins[k]))
+        if st == 0:
+            out.append(int(mat[k].searchsorted(rng.random(), side="right")))
+        elif st == 1:
+            out.append(int(ins[k].searchsorted(rng.random(), side="right")))
         if k >= kend:
             break
-        t = p.t[k]
-        if st == "M":
-            nxt = rng.choice(3, p=t[0:3] / t[0:3].sum())
-            st, k = ("M", k + 1) if nxt == 0 else ("I", k) if nxt == 1 else ("D", k + 1)
-        elif st == "I":
-            nxt = rng.choice(2, p=t[3:5] / t[3:5].sum())
-            st, k = ("M", k + 1) if nxt == 0 else ("I", k)
+        if st == 0:
+            nxt = int(tm[k].searchsorted(rng.random(), side="right"))
+            st, k = (0, k + 1) if nxt == 0 else (1, k) if nxt == 1 else (2, k + 1)
+        elif st == 1:
+            nxt = int(ti[k].searchsorted(rng.random(), side="right"))
+            st, k = (0, k + 1) if nxt == 0 else (1, k)
         else:
-            nxt = rng.choice(2, p=t[5:7] / t[5:7].sum())
-            st, k = ("M", k + 1) if nxt == 0 else ("D", k + 1)
+            nxt = int(td[k].searchsorted(rng.random(), side="right"))
+            st, k = (0, k + 1) if nxt == 0 else (2, k + 1)
     return np.array(out, dtype=np.uint8)
 
 
@@ -259,10 +282,13 @@ class Workload:
         return "".join(profile_text(p) for p in self.profiles)
 
 
-def make_config(idx, scale=1.0, scorer=None, seed=None, calib_rng_seed=7):
+def make_config(idx, scale=1.0, scorer=None, seed=None, calib_rng_seed=7, genomes=None):
     """Build benchmark config `idx` (0..4).  scale < 1 shrinks the counts of
-    profiles and targets (never their lengths) for quick tests."""
+    profiles and targets (never their lengths) for quick tests.  For the
+    marker-set config (2), `genomes` keeps only the first n genomes of the
+    full draw (the same profiles and the same first n genomes)."""
     rng = np.random.default_rng(1000 + idx if seed is None else seed)
+    genomes_keep = genomes
     profiles, targets, ids, pairs, truth = [], [], [], None, {}
     if idx == 0:
         profiles = [sample_profile(rng, 100, "synth0_p0")]
@@ -306,7 +332,7 @@ def make_config(idx, scale=1.0, scorer=None, seed=None, calib_rng_seed=7):
         ms = rng.integers(200, 1501, size=npf)
         profiles = [sample_profile(rng, int(m), f"marker{i}") for i, m in enumerate(ms)]
         genomes = []
-        for g in range(ngen):
+        for g in range(ngen if genomes_keep is None else min(ngen, genomes_keep)):
             ls = lognormal_lengths(rng, nper, 280, SIGMA_L, 30, 4000)
             prots = [background_seq(rng, int(x)) for x in ls]
             for pi in range(npf):

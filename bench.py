@@ -379,7 +379,7 @@ def adjoint_run(sxhmm, eng, torch):
                     "out (the caller's, reused across calls), copies included"}
 
 
-def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True):
+def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True, envelopes="auto", traces="auto"):
     """The marker-set configuration as BUSCO and EukCC issue it
     (src/busco/mod.rs:297-304, src/eukcc/mod.rs:77): 250 marker profiles
     (M uniform 200-1,500) against one genome of 4,000 proteins at a time
@@ -395,7 +395,7 @@ def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True):
     cache = os.environ.get("SXHMM_BENCH_CACHE", "/tmp/sxhmm_bench_cache")
     os.makedirs(cache, exist_ok=True)
     key = os.path.join(cache, f"cfg2_g{ngenomes}.npz")
-    eng = sxhmm.Engine(device=local, prescreen=prescreen)
+    eng = sxhmm.Engine(device=local, prescreen=prescreen, envelopes=envelopes, traces=traces)
     t0 = time.time()
     if os.path.exists(key):
         z = np.load(key, allow_pickle=False)
@@ -427,6 +427,7 @@ def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True):
     ts.close()
     walls, launches, hits, cells = [], [], 0, 0.0
     stage = np.zeros(8)
+    pin, pout = np.zeros(8), np.zeros(8)
     pre_ms = res_ms = 0.0
     for g in range(len(gen)):
         sg, og, lg = genome(g)
@@ -438,6 +439,8 @@ def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True):
         ts.close()
         st = eng.stats()
         stage += np.array(st["ms"])
+        pin += np.array(st["pairs_in"])
+        pout += np.array(st["pairs_out"])
         pre_ms += st["prescreen"]["ms"]
         res_ms += st["prescreen"]["rescore_ms"]
         launches.append(st["kernel_launches"])
@@ -459,6 +462,9 @@ def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True):
             "stage_ms_per_genome": per,
             "prescreen_ms_per_genome": round(pre_ms / ng, 2), "rescore_ms_per_genome": round(res_ms / ng, 2),
             "launches_per_genome": int(statistics.median(launches)),
+            "per_genome": {"final_pairs": round(pin[4] / ng, 1), "envelopes_on_device": round(pout[5] / ng, 1),
+                           "regions_to_device": round(pin[6] / ng, 1), "regions_traced_on_device": round(pout[6] / ng, 1)},
+            "placement": {"envelopes": envelopes, "traces": traces},
             "host_gap_ms_per_genome": round(wall - critical, 2),
             "host_gap_note": "median wall (target upload + search + hits) minus the device stages on the critical "
                              "path (MSV, bias, Viterbi, Forward pre-screen, row passes) and the host tail: an upper "
@@ -602,7 +608,19 @@ def main():
             torch.cuda.synchronize()
             ptimes.append(ev0.elapsed_time(ev1))
         pst = peng.stats()
+        # end to end as the batched arm's e2e: the targets copied from pinned
+        # host memory, the search, the hits read back
+        flush_l2(torch, l2)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        pts2 = peng.targets_digital(pinned, offs, lens)
+        phits2, pdoms2 = peng.search(pps, pts2, cfg)
+        torch.cuda.synchronize()
+        pe2e_ms = (time.perf_counter() - t) * 1e3
+        pts2.close()
         plain = {"value": cells / (max(ptimes) / 1e3) / 1e9, "ms_per_step": max(ptimes), "hits": len(phits),
+                 "e2e": {"value": cells / (pe2e_ms / 1e3) / 1e9, "unit": "GCUPS", "ms": round(pe2e_ms, 1),
+                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": len(phits2) * 48 + len(pdoms2) * 56},
                  "stage_ms": {k: round(v, 3) for k, v in zip(STAGES, pst["ms"])},
                  "what": "one 128-thread CTA per pair, row split across threads, shared-memory exchange + "
                          "__syncthreads per row, block max-reduction, Viterbi D chain by one thread; same "
@@ -694,6 +712,7 @@ def main():
     if plain is not None:
         line["plain"] = plain
         line["batched_over_plain"] = plain["ms_per_step"] / ms_step
+        line["batched_over_plain_e2e"] = plain["e2e"]["ms"] / e2e_ms
     if rank == 0 and not args.no_cpu_baseline and ws == 1:
         progress("oracle leg (CPU baseline + full-size parity)")
         line["cpu_baseline"], line["parity"] = oracle_leg(eng, ps, text, seq, offs, lens)

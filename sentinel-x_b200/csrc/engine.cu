@@ -24,6 +24,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -58,6 +59,27 @@ thread_local std::string g_err;
 struct NvtxRange {
   explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
   ~NvtxRange() { nvtxRangePop(); }
+};
+
+// Wall-clock phases of one sx_search, printed to stderr when the environment
+// variable SXHMM_PROFILE is set (a diagnostic for tuning placements; it adds
+// clock reads only).
+struct PhaseLog {
+  bool on = std::getenv("SXHMM_PROFILE") != nullptr;
+  std::vector<std::pair<std::string, double>> v;
+  void add(const char* name, std::chrono::steady_clock::time_point t0) {
+    if (on) v.emplace_back(name, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+  }
+  void print() const {
+    if (!on) return;
+    std::string o = "[sxhmm profile]";
+    char buf[96];
+    for (const auto& p : v) {
+      snprintf(buf, sizeof buf, " %s=%.1fms", p.first.c_str(), p.second);
+      o += buf;
+    }
+    fprintf(stderr, "%s\n", o.c_str());
+  }
 };
 
 int fail(int code, const std::string& msg) {
@@ -367,6 +389,25 @@ struct Streams {
   }
 };
 
+// Set once a host job has copied a slot's row buffers out; the engine thread
+// waits for it before it reuses those buffers for a later block.
+struct RowsTicket {
+  std::mutex mu;
+  std::condition_variable cv;
+  bool done = false;
+  void set() {
+    {
+      std::lock_guard<std::mutex> g(mu);
+      done = true;
+    }
+    cv.notify_all();
+  }
+  void wait() {
+    std::unique_lock<std::mutex> g(mu);
+    cv.wait(g, [&] { return done; });
+  }
+};
+
 // Streams, events and survivor lists of one block of a search.  A search
 // keeps two blocks in flight: block b+1's MSV runs on one slot while block
 // b's later stages, row passes and host re-check use the other.  MSV goes to
@@ -389,6 +430,17 @@ struct Slot {
   DevBuf<int32_t> rlist;           // pre-screen survivors: target indices, rcap per profile of the block
   DevBuf<unsigned> rcount;         // survivors per profile of the block
   cudaEvent_t pre_done = nullptr;  // pre-screen finished (its time, for the stats)
+  // Forward/Backward row passes of the block's final pairs, in buffers of
+  // their own: the engine thread queues them and moves on to the next block;
+  // a host job waits for them, copies the rows out and releases the buffers.
+  DevBuf<PairRec> rrecs;
+  DevBuf<BinRegion> rbins;
+  DevBuf<unsigned> rcnt;
+  DevBuf<int64_t> roff;
+  DevBuf<float> rows_f, rows_b;
+  cudaEvent_t rows_t0 = nullptr, rows_t1 = nullptr;
+  cudaStream_t rows_copy = nullptr;  // device-to-host copies of the rows (host job)
+  std::shared_ptr<RowsTicket> rows_busy;
   void create() {
     int least = 0, greatest = 0;
     CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -400,6 +452,9 @@ struct Slot {
     lo.create(least, 5);
     for (auto& e : ev) CK(cudaEventCreate(&e));
     CK(cudaEventCreate(&pre_done));
+    CK(cudaEventCreate(&rows_t0));
+    CK(cudaEventCreate(&rows_t1));
+    CK(cudaStreamCreateWithFlags(&rows_copy, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&msv_done, cudaEventDisableTiming));
   }
   void destroy() {
@@ -409,6 +464,13 @@ struct Slot {
       if (e) cudaEventDestroy(e);
     if (msv_done) cudaEventDestroy(msv_done);
     if (pre_done) cudaEventDestroy(pre_done);
+    if (rows_busy) rows_busy->wait();
+    if (rows_t0) cudaEventDestroy(rows_t0);
+    if (rows_t1) cudaEventDestroy(rows_t1);
+    if (rows_copy) {
+      cudaStreamSynchronize(rows_copy);
+      cudaStreamDestroy(rows_copy);
+    }
   }
 };
 
@@ -1040,6 +1102,94 @@ void rows_pass_sync(sx_engine* E, const sx_profiles* P, const sx_targets* T, con
   });
 }
 
+// Row passes of a block's final pairs queued without waiting: when all of
+// their rows fit one chunk, the kernels go to slot S's high-priority streams
+// with the slot's own row buffers and the call returns a fetch function; a
+// host job calls it, which waits for the kernels, copies the rows out on the
+// slot's copy stream, adds the passes' device time to *dev_ms and releases
+// the buffers.  Returns an empty function when the rows need more than one
+// chunk (the caller then takes the synchronous rows_pass).
+std::function<RowsChunk()> rows_pass_async(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T,
+                                           const std::vector<FinalPair>& pairs, std::mutex* ms_mu, double* dev_ms) {
+  const auto& K = kernels();
+  const int64_t row_budget = std::max<int64_t>(scratch_budget(E, E->batch_bytes / 2) / (int64_t)sizeof(float), 1 << 20);
+  int64_t ro = 0;
+  for (const FinalPair& f : pairs) ro += 6 * ((int64_t)T->len[f.t] + 1);
+  if (pairs.empty() || ro > row_budget) return {};
+  if (S.rows_busy) S.rows_busy->wait();  // an earlier block's rows are still being read
+  std::vector<std::vector<size_t>> byb(kNumVbins);
+  for (size_t i = 0; i < pairs.size(); i++) byb[P->dp[pairs[i].p].vbin].push_back(i);
+  std::vector<PairRec> recs;
+  auto c = std::make_shared<RowsChunk>();
+  std::vector<BinRegion> reg(kNumVbins);
+  std::vector<unsigned> cnt(kNumVbins, 0);
+  ro = 0;
+  for (int b = 0; b < kNumVbins; b++) {
+    reg[b].off = (int64_t)recs.size();
+    reg[b].cap = (uint32_t)byb[b].size();
+    reg[b].pad = 0;
+    cnt[b] = (unsigned)byb[b].size();
+    for (size_t i : byb[b]) {
+      const FinalPair& f = pairs[i];
+      recs.push_back({f.p, f.t, f.usc, f.filtersc, f.vsc, 0.f, f.slot, 0});
+      c->off.push_back(ro);
+      c->which.push_back(i);
+      ro += 6 * ((int64_t)T->len[f.t] + 1);
+    }
+  }
+  cudaStream_t s = S.hi.main;
+  S.rrecs.upload(recs.data(), recs.size(), s);
+  S.roff.upload(c->off.data(), c->off.size(), s);
+  S.rbins.upload(reg.data(), reg.size(), s);
+  S.rcnt.upload(cnt.data(), cnt.size(), s);
+  S.rows_f.alloc((size_t)ro);
+  S.rows_b.alloc((size_t)ro);
+  CK(cudaEventRecord(S.rows_t0, s));
+  // rows the kernels never touch are zero
+  CK(cudaMemsetAsync(S.rows_f.p, 0, sizeof(float) * (size_t)ro, s));
+  CK(cudaMemsetAsync(S.rows_b.p, 0, sizeof(float) * (size_t)ro, s));
+  fork_aux(S.hi);
+  for (int b = 0; b < kNumVbins; b++) {
+    if (!cnt[b]) continue;
+    const int blocks = warp_ctas(E->num_sms, cnt[b]);
+    cudaStream_t sa = S.hi.aux[(2 * b) % S.hi.naux], sb = S.hi.aux[(2 * b + 1) % S.hi.naux];
+    K.fwd[b]<<<blocks, 32, 0, sa>>>(S.rrecs.p, S.rcnt.p, S.rbins.p, b, nullptr, nullptr, nullptr, S.overflow.p,
+                                     P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p, T->d_len.p,
+                                     T->d_xsc.p, 0.f, S.rows_f.p, S.roff.p);
+    K.bwd[b]<<<blocks, 32, 0, sb>>>(S.rrecs.p, S.rcnt.p, S.rbins.p, b, P->d_prof.p, P->d_vfb.p, T->d_res.p,
+                                     T->d_off.p, T->d_len.p, T->d_xsc.p, S.rows_b.p, S.roff.p);
+    E->stats.kernel_launches += 2;
+  }
+  CK(cudaGetLastError());
+  join_aux(S.hi);
+  CK(cudaEventRecord(S.rows_t1, s));
+  auto ticket = std::make_shared<RowsTicket>();
+  S.rows_busy = ticket;
+  Slot* SP = &S;
+  const int device = E->device;
+  return [SP, c, ro, ticket, ms_mu, dev_ms, device]() -> RowsChunk {
+    struct Release {  // the buffers are free again, even if a copy failed
+      RowsTicket& t;
+      ~Release() { t.set(); }
+    } rel{*ticket};
+    Slot& S = *SP;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamWaitEvent(S.rows_copy, S.rows_t1, 0));
+    c->f.resize((size_t)ro);
+    c->b.resize((size_t)ro);
+    CK(cudaMemcpyAsync(c->f.data(), S.rows_f.p, sizeof(float) * (size_t)ro, cudaMemcpyDeviceToHost, S.rows_copy));
+    CK(cudaMemcpyAsync(c->b.data(), S.rows_b.p, sizeof(float) * (size_t)ro, cudaMemcpyDeviceToHost, S.rows_copy));
+    CK(cudaStreamSynchronize(S.rows_copy));
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, S.rows_t0, S.rows_t1) != cudaSuccess) cudaGetLastError();
+    {
+      std::lock_guard<std::mutex> g(*ms_mu);
+      *dev_ms += ms;
+    }
+    return std::move(*c);
+  };
+}
+
 // Background host work: one driver thread runs the queued jobs in order, each
 // over `threads` workers, while the engine thread keeps the device busy with
 // later profile blocks.
@@ -1402,7 +1552,7 @@ struct EnvSource {
 };
 
 int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T, std::vector<EnvSource>& srcs,
-                        int nthr) {
+                        int nthr, PhaseLog* plog = nullptr) {
   // every request of every batch, as (batch, request)
   std::vector<std::pair<uint32_t, uint32_t>> items;
   for (size_t b = 0; b < srcs.size(); b++) {
@@ -1457,6 +1607,7 @@ int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T,
       b++;
     }
     const size_t n = b - a;
+    const auto tb0 = std::chrono::steady_clock::now();
     E->env_recs.upload(recs.data(), n, s);
     E->env_planes.alloc((size_t)planes);
     E->env_rows.alloc((size_t)rowsz);
@@ -1491,6 +1642,8 @@ int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T,
     std::vector<float> hrows((size_t)rowsz);
     CK(cudaMemcpyAsync(hrows.data(), E->env_rows.p, sizeof(float) * (size_t)rowsz, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (plog) plog->add("env_fb_pass", tb0);
+    const auto tb1 = std::chrono::steady_clock::now();
     parallel_for(n, nthr, [&](size_t x) {
       const sxk::EnvRec& r = recs[x];
       const auto& it = items[order[a + x]];
@@ -1509,6 +1662,8 @@ int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T,
       std::copy(f.pc.begin(), f.pc.end(), haux.begin() + r.aux_off + 2 * w);
       std::copy(f.fac.begin(), f.fac.end(), hfac.begin() + r.fac_off);
     }
+    if (plog) plog->add("env_factors_host", tb1);
+    const auto tb2 = std::chrono::steady_clock::now();
     CK(cudaMemcpyAsync(E->env_aux.p, haux.data(), sizeof(float) * (size_t)aux, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(E->env_fac.p, hfac.data(), sizeof(double) * (size_t)fac, cudaMemcpyHostToDevice, s));
     each_bin([&](int vb, int x0, int cnt, int blocks) {
@@ -1520,6 +1675,7 @@ int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T,
     std::vector<float> hout(n * sxk::kEnvOut);
     CK(cudaMemcpyAsync(hout.data(), E->env_out.p, sizeof(float) * hout.size(), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (plog) plog->add("env_post_pass", tb2);
     for (size_t x = 0; x < n; x++) {
       const float* o = hout.data() + x * sxk::kEnvOut;
       EnvDeviceOut& d = out_of(order[a + x]);
@@ -2106,13 +2262,15 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     const double waves = std::ceil((double)regs.size() / (20.0 * E->num_sms));
     return cells * 19e-6 / std::max(1, nthr) > 30.0 + waves * chain;
   };
+  std::mutex rows_ms_mu;
   auto rows_and_queue = [&](Slot& S, BlockOut* B, bool dev_env) {
     B->res.resize(B->finals.size());
-    const auto t0 = std::chrono::steady_clock::now();
-    rows_pass(E, S, P, T, B->finals, [&, B, dev_env](RowsChunk&& c) {
-      auto ch = std::make_shared<RowsChunk>(std::move(c));
-      hq.push([&, B, ch, dev_env](int nthr) {
+    // the host job of one chunk of rows: `get` hands it the rows (at once, or
+    // after waiting for the asynchronous row passes)
+    auto queue_chunk = [&, B, dev_env](std::function<RowsChunk()> get) {
+      hq.push([&, B, dev_env, get](int nthr) {
         try {
+          auto ch = std::make_shared<RowsChunk>(get());
           const size_t nq = ch->which.size();
           // largest pairs first, for an even finish across the workers
           std::vector<size_t> ord(nq);
@@ -2184,8 +2342,21 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
           }
         }
       });
+    };
+    auto fetch = rows_pass_async(E, S, P, T, B->finals, &rows_ms_mu, &rows_ms);
+    if (fetch) {
+      queue_chunk(std::move(fetch));
+      return;
+    }
+    // rows larger than one chunk: passes in turn, each chunk queued as it arrives
+    const auto t0 = std::chrono::steady_clock::now();
+    rows_pass(E, S, P, T, B->finals, [&](RowsChunk&& c) {
+      auto ch = std::make_shared<RowsChunk>(std::move(c));
+      queue_chunk([ch]() { return std::move(*ch); });
     });
-    rows_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    std::lock_guard<std::mutex> g(rows_ms_mu);
+    rows_ms += ms;
   };
 
   std::vector<int> unfiltered;
@@ -2224,7 +2395,10 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     rows_and_queue(E->sl[0], B, !(E->flags & SX_FLAG_ENV_HOST));  // every pair reaches domain definition
   }
   const auto t_dev = std::chrono::steady_clock::now();
+  PhaseLog plog;
+  plog.add("cascade_and_rows", t_start);
   E->stats.ms[5] = hq.finish();
+  plog.add("host_pool_drain", t_dev);
   if (host_err_code) return fail(host_err_code, host_err_msg);
   // every multi-domain region's trace ensemble, then every envelope of the
   // search through the device passes at once, on an idle GPU, then each
@@ -2236,6 +2410,7 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     for (auto& pb : pending)
       if (pb->dev_regions) rsrc.push_back({pb->db.get(), &pb->db->regions()});
     rstats = region_passes(E, P, T, rsrc, E->host_threads);
+    plog.add("region_passes", t_env);
     env_launches += rstats.launches;
     for (auto& pb : pending) {
       pb->reqs = pb->db->requests();
@@ -2243,7 +2418,10 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     }
     std::vector<EnvSource> srcs;
     for (auto& pb : pending) srcs.push_back({pb->db.get(), &pb->reqs, &pb->F, &pb->D});
-    env_launches += envelope_passes(E, P, T, srcs, E->host_threads);
+    const auto t_ep = std::chrono::steady_clock::now();
+    env_launches += envelope_passes(E, P, T, srcs, E->host_threads, &plog);
+    plog.add("envelope_passes", t_ep);
+    const auto t_fin = std::chrono::steady_clock::now();
     std::vector<std::pair<PendingBatch*, size_t>> todo;
     for (auto& pb : pending)
       for (size_t q = 0; q < pb->which.size(); q++)
@@ -2254,6 +2432,7 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
       const size_t i = pb.which[q];
       pb.B->res[i].hit = pb.db->finish(q, pb.F, pb.D, pb.B->res[i].h);
     });
+    plog.add("finish", t_fin);
     E->stats.ms[5] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_env).count();
   }
   // profiles longer than kMaxM: MSV on the device, the exact host checks of the
@@ -2332,6 +2511,8 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
   E->stats.ms[4] = rows_ms;
   E->stats.ms[6] = std::chrono::duration<double, std::milli>(t_end - t_start).count();
   E->stats.ms[7] = std::chrono::duration<double, std::milli>(t_end - t_dev).count();
+  plog.add("total", t_start);
+  plog.print();
   std::vector<std::vector<std::pair<int32_t, HitOut>>> per(np);
   for (auto& B : outs) {
     for (const auto& f : B->finals) E->stats.cells[4] += (double)P->h[f.p].m * T->len[f.t];

@@ -379,7 +379,7 @@ def adjoint_run(sxhmm, eng, torch):
                     "out (the caller's, reused across calls), copies included"}
 
 
-def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True, envelopes="auto", traces="auto"):
+def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True, envelopes="auto", traces="auto", batch_bytes=0):
     """The marker-set configuration as BUSCO and EukCC issue it
     (src/busco/mod.rs:297-304, src/eukcc/mod.rs:77): 250 marker profiles
     (M uniform 200-1,500) against one genome of 4,000 proteins at a time
@@ -395,7 +395,7 @@ def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True, envelopes="aut
     cache = os.environ.get("SXHMM_BENCH_CACHE", "/tmp/sxhmm_bench_cache")
     os.makedirs(cache, exist_ok=True)
     key = os.path.join(cache, f"cfg2_g{ngenomes}.npz")
-    eng = sxhmm.Engine(device=local, prescreen=prescreen, envelopes=envelopes, traces=traces)
+    eng = sxhmm.Engine(device=local, prescreen=prescreen, envelopes=envelopes, traces=traces, batch_bytes=batch_bytes)
     t0 = time.time()
     if os.path.exists(key):
         z = np.load(key, allow_pickle=False)

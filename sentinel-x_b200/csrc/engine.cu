@@ -1109,6 +1109,7 @@ void rows_pass_sync(sx_engine* E, const sx_profiles* P, const sx_targets* T, con
 // slot's copy stream, adds the passes' device time to *dev_ms and releases
 // the buffers.  Returns an empty function when the rows need more than one
 // chunk (the caller then takes the synchronous rows_pass).
+constexpr int kRowsWarps = 8;  // warps (pairs) per CTA of the asynchronous row passes
 std::function<RowsChunk()> rows_pass_async(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T,
                                            const std::vector<FinalPair>& pairs, std::mutex* ms_mu, double* dev_ms) {
   const auto& K = kernels();
@@ -1119,6 +1120,10 @@ std::function<RowsChunk()> rows_pass_async(sx_engine* E, Slot& S, const sx_profi
   if (S.rows_busy) S.rows_busy->wait();  // an earlier block's rows are still being read
   std::vector<std::vector<size_t>> byb(kNumVbins);
   for (size_t i = 0; i < pairs.size(); i++) byb[P->dp[pairs[i].p].vbin].push_back(i);
+  // longest first: the warps of a CTA then carry similar lengths, and the
+  // longest chains start first
+  for (auto& v : byb)
+    std::stable_sort(v.begin(), v.end(), [&](size_t a, size_t b) { return T->len[pairs[a].t] > T->len[pairs[b].t]; });
   std::vector<PairRec> recs;
   auto c = std::make_shared<RowsChunk>();
   std::vector<BinRegion> reg(kNumVbins);
@@ -1151,12 +1156,16 @@ std::function<RowsChunk()> rows_pass_async(sx_engine* E, Slot& S, const sx_profi
   fork_aux(S.hi);
   for (int b = 0; b < kNumVbins; b++) {
     if (!cnt[b]) continue;
-    const int blocks = warp_ctas(E->num_sms, cnt[b]);
+    // The row passes are latency-bound chains that run for milliseconds
+    // beside the next block's MSV: packed kRowsWarps to a CTA they hold the
+    // registers of a few SMs instead of one MSV CTA slot on nearly every SM.
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)cnt[b] + kRowsWarps - 1) / kRowsWarps,
+                                                                   (int64_t)E->num_sms * 32 / kRowsWarps));
     cudaStream_t sa = S.hi.aux[(2 * b) % S.hi.naux], sb = S.hi.aux[(2 * b + 1) % S.hi.naux];
-    K.fwd[b]<<<blocks, 32, 0, sa>>>(S.rrecs.p, S.rcnt.p, S.rbins.p, b, nullptr, nullptr, nullptr, S.overflow.p,
+    K.fwd[b]<<<blocks, 32 * kRowsWarps, 0, sa>>>(S.rrecs.p, S.rcnt.p, S.rbins.p, b, nullptr, nullptr, nullptr, S.overflow.p,
                                      P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p, T->d_len.p,
                                      T->d_xsc.p, 0.f, S.rows_f.p, S.roff.p);
-    K.bwd[b]<<<blocks, 32, 0, sb>>>(S.rrecs.p, S.rcnt.p, S.rbins.p, b, P->d_prof.p, P->d_vfb.p, T->d_res.p,
+    K.bwd[b]<<<blocks, 32 * kRowsWarps, 0, sb>>>(S.rrecs.p, S.rcnt.p, S.rbins.p, b, P->d_prof.p, P->d_vfb.p, T->d_res.p,
                                      T->d_off.p, T->d_len.p, T->d_xsc.p, S.rows_b.p, S.roff.p);
     E->stats.kernel_launches += 2;
   }
@@ -1569,7 +1578,10 @@ int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T,
   auto out_of = [&](size_t x) -> EnvDeviceOut& { return (*srcs[items[x].first].D)[items[x].second]; };
   const auto& K = kernels();
   cudaStream_t s = E->env_stream;
-  const int64_t budget = scratch_budget(E, std::max<int64_t>(E->batch_bytes / 2, 256LL << 20));
+  // Planes of every envelope of a search at once when they fit: each batch
+  // is one round of latency-bound passes (the longest envelope sets its
+  // time) plus a host round trip, so fewer, larger batches finish sooner.
+  const int64_t budget = scratch_budget(E, std::max<int64_t>(4 * E->batch_bytes, 256LL << 20));
   std::vector<size_t> order(nr);
   std::iota(order.begin(), order.end(), (size_t)0);
   std::stable_sort(order.begin(), order.end(),
@@ -1667,7 +1679,9 @@ int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T,
     CK(cudaMemcpyAsync(E->env_aux.p, haux.data(), sizeof(float) * (size_t)aux, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(E->env_fac.p, hfac.data(), sizeof(double) * (size_t)fac, cudaMemcpyHostToDevice, s));
     each_bin([&](int vb, int x0, int cnt, int blocks) {
-      K.envp[vb]<<<blocks, 32, 0, s>>>(E->env_recs.p + x0, cnt, P->d_prof.p, P->d_vfb.p, E->env_planes.p,
+      const size_t psm = sxk::env_post_smem(kVcBins[vb]);
+      CK(cudaFuncSetAttribute((const void*)K.envp[vb], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+      K.envp[vb]<<<blocks, 32, psm, s>>>(E->env_recs.p + x0, cnt, P->d_prof.p, P->d_vfb.p, E->env_planes.p,
                                        E->env_aux.p, E->env_fac.p, E->env_out.p);
       launches += 1;
     });

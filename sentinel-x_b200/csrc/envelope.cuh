@@ -395,6 +395,29 @@ __global__ void __launch_bounds__(32) env_backward_kernel(const EnvRec* __restri
   }
 }
 
+// Per-lane column arrays of a warp-per-envelope kernel: registers for narrow
+// profiles, shared memory for wide ones (VC >= kPostSmemVC), where holding
+// the post kernel's 17 arrays of VC floats in registers spills to local memory.
+// In shared memory element c of a lane's array sits at s[32 * c]: a warp's
+// access to one c is one conflict-free wavefront.
+template <int VC, bool SH>
+struct Cols {
+  float r[SH ? 1 : VC];
+  float* s;
+  __device__ __forceinline__ float& operator[](int c) {
+    if constexpr (SH) return s[c * 32];
+    else return r[c];
+  }
+};
+constexpr int kPostSmemVC = 16;
+constexpr int kPostArrays = 17;  // tp[8], sm, omp, oip, odp, pm, pi, om, oi, od
+// Dynamic shared memory of env_post_kernel<VC> (one warp per CTA): the row
+// buffer of the insert-posterior sum, then the column arrays when they live
+// in shared memory.
+__host__ __device__ constexpr size_t env_post_smem(int vc) {
+  return ((vc >= kPostSmemVC ? (size_t)kPostArrays : 0) + 1) * 32 * vc * sizeof(float);
+}
+
 __device__ __forceinline__ float oa_gate(float t, float v) { return t > 0.0f ? v : 0.0f; }
 __device__ __forceinline__ float oa_dis(float t, float v) { return t == 0.0f ? SX_NEG_INF : v; }
 
@@ -440,12 +463,28 @@ __global__ void __launch_bounds__(32) env_post_kernel(const EnvRec* __restrict__
                pmove0 = r.pmove == 0.0f;
     // probability transitions at column k: p_bm[k], p_mm[k-1], p_im[k-1], p_dm[k-1],
     // p_mi[k], p_ii[k], p_md[k-1], p_dd[k-1]
-    float tp[8][VC];
+    constexpr bool SH = VC >= kPostSmemVC;
+    extern __shared__ float post_smem[];
+    Cols<VC, SH> tp[8], sm, omp, oip, odp, pm, pi, om, oi, od;
+    float* sirow = post_smem;  // the row's insert posteriors, element (c, lane) at c * 32 + lane
+    if constexpr (SH) {
+      float* b = post_smem + 32 * VC + lane;
+#pragma unroll
+      for (int q = 0; q < 8; q++) tp[q].s = b + q * 32 * VC;
+      sm.s = b + 8 * 32 * VC;
+      omp.s = b + 9 * 32 * VC;
+      oip.s = b + 10 * 32 * VC;
+      odp.s = b + 11 * 32 * VC;
+      pm.s = b + 12 * 32 * VC;
+      pi.s = b + 13 * 32 * VC;
+      om.s = b + 14 * 32 * VC;
+      oi.s = b + 15 * 32 * VC;
+      od.s = b + 16 * 32 * VC;
+    }
 #pragma unroll
     for (int q = 0; q < 8; q++)
 #pragma unroll
       for (int c = 0; c < VC; c++) tp[q][c] = img.at(kRowFwd + q, c, lane);
-    float sm[VC], omp[VC], oip[VC], odp[VC];
 #pragma unroll
     for (int c = 0; c < VC; c++) {
       sm[c] = 0.f;
@@ -461,7 +500,6 @@ __global__ void __launch_bounds__(32) env_post_kernel(const EnvRec* __restrict__
     }
     for (int i = 1; i <= L; i++) {
       const double f = fac[i];
-      float pm[VC], pi[VC];
 #pragma unroll
       for (int c = 0; c < VC; c++) {
         const int k = lane * VC + c + 1;
@@ -470,20 +508,27 @@ __global__ void __launch_bounds__(32) env_post_kernel(const EnvRec* __restrict__
         pi[c] = k < M ? (float)__dmul_rn(__dmul_rn((double)FI[e], (double)OI[e]), f) : 0.f;
         if (k <= M) sm[c] = fadd(sm[c], pm[c]);
       }
-      // si: every insert posterior, row-major in k
-      for (int sl = 0; sl < nl; sl++) {
-        if (lane == sl) {
+      // si: every insert posterior, row-major in k.  The row's values go to
+      // shared memory and lane 0 adds them in column order (the same order
+      // and roundings as a lane-to-lane baton, without its 32 shuffle hops).
 #pragma unroll
-          for (int c = 0; c < VC; c++)
-            if (lane * VC + c + 1 <= M) si = fadd(si, pi[c]);
+      for (int c = 0; c < VC; c++) sirow[c * 32 + lane] = pi[c];
+      __syncwarp();
+      if (lane == 0) {
+        int c = 0, l = 0;
+        for (int k = 1; k <= M; k++) {
+          si = fadd(si, sirow[c * 32 + l]);
+          if (++c == VC) {
+            c = 0;
+            l++;
+          }
         }
-        si = __shfl_sync(kFull, si, sl);
       }
+      __syncwarp();
       // OA row: M and I from the previous row, then the D chain in order
       const float oml0 = __shfl_up_sync(kFull, omp[VC - 1], 1);
       const float oil0 = __shfl_up_sync(kFull, oip[VC - 1], 1);
       const float odl0 = __shfl_up_sync(kFull, odp[VC - 1], 1);
-      float om[VC], oi[VC], od[VC];
       float emax = SX_NEG_INF;
 #pragma unroll
       for (int c = 0; c < VC; c++) {
@@ -505,26 +550,57 @@ __global__ void __launch_bounds__(32) env_post_kernel(const EnvRec* __restrict__
         }
       }
       const float omleft0 = __shfl_up_sync(kFull, om[VC - 1], 1);
-      float dcar = SX_NEG_INF;
-      for (int sl = 0; sl < nl; sl++) {
-        if (lane == sl) {
+      // The D chain od[k] = max(gate(t_md, om[k-1]), gate(t_dd, od[k-1])) only
+      // selects and takes maxima of non-negative values (or -inf), exact in
+      // any order, so it runs as a scan.  Column k maps the chain value v to
+      // max(a_k, v) when t_dd > 0 and to the constant max(a_k, 0) otherwise
+      // (k = 1: the constant -inf; k > M: the identity).  Each lane composes
+      // its columns' maps, the composites are scanned across lanes (5 shuffle
+      // rounds), and each lane replays its columns from its carry.
+      bool lc = false;          // the lane's composite: constant (true) or v -> max(lv, v)
+      float lv = SX_NEG_INF;
 #pragma unroll
-          for (int c = 0; c < VC; c++) {
-            const int k = lane * VC + c + 1;
-            if (k > M) {
-              od[c] = SX_NEG_INF;
-            } else if (k == 1) {
-              od[c] = SX_NEG_INF;
-              dcar = SX_NEG_INF;
-            } else {
-              const float omk1 = c ? om[c - 1] : omleft0;
-              od[c] = fmaxf(oa_gate(tp[6][c], omk1), oa_gate(tp[7][c], dcar));
-              dcar = od[c];
-              emax = fmaxf(emax, od[c]);
-            }
-          }
+      for (int c = 0; c < VC; c++) {
+        const int k = lane * VC + c + 1;
+        if (k > M) continue;
+        if (k == 1) {
+          lc = true;
+          lv = SX_NEG_INF;
+          continue;
         }
-        dcar = __shfl_sync(kFull, dcar, sl);
+        const float a = oa_gate(tp[6][c], c ? om[c - 1] : omleft0);
+        if (tp[7][c] > 0.0f) {
+          lv = fmaxf(lv, a);
+        } else {
+          lc = true;
+          lv = fmaxf(a, 0.0f);
+        }
+      }
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {  // inclusive scan: earlier lanes' composite, then this lane's
+        const int pc = __shfl_up_sync(kFull, (int)lc, o);
+        const float pv = __shfl_up_sync(kFull, lv, o);
+        if (lane >= o && !lc) {
+          lv = fmaxf(pv, lv);
+          lc = pc != 0;
+        }
+      }
+      float dcar = __shfl_up_sync(kFull, lv, 1);  // chain value entering this lane's first column
+      if (lane == 0) dcar = SX_NEG_INF;
+#pragma unroll
+      for (int c = 0; c < VC; c++) {
+        const int k = lane * VC + c + 1;
+        if (k > M) {
+          od[c] = SX_NEG_INF;
+        } else if (k == 1) {
+          od[c] = SX_NEG_INF;
+          dcar = SX_NEG_INF;
+        } else {
+          const float omk1 = c ? om[c - 1] : omleft0;
+          od[c] = fmaxf(oa_gate(tp[6][c], omk1), oa_gate(tp[7][c], dcar));
+          dcar = od[c];
+          emax = fmaxf(emax, od[c]);
+        }
       }
       if (lane >= nl) {
 #pragma unroll

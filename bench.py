@@ -428,7 +428,7 @@ def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True, envelopes="aut
     walls, launches, hits, cells = [], [], 0, 0.0
     stage = np.zeros(8)
     pin, pout = np.zeros(8), np.zeros(8)
-    pre_ms = res_ms = 0.0
+    pre_ms = res_ms = vpre_ms = 0.0
     for g in range(len(gen)):
         sg, og, lg = genome(g)
         torch.cuda.synchronize()
@@ -443,6 +443,7 @@ def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True, envelopes="aut
         pout += np.array(st["pairs_out"])
         pre_ms += st["prescreen"]["ms"]
         res_ms += st["prescreen"]["rescore_ms"]
+        vpre_ms += st["vprescreen"]["ms"]
         launches.append(st["kernel_launches"])
         hits += len(h)
         cells += float(ms.sum()) * float(lg.sum())
@@ -461,6 +462,7 @@ def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True, envelopes="aut
             "wall_ms_per_genome": {"median": round(wall, 2), "min": round(min(walls), 2), "max": round(max(walls), 2)},
             "stage_ms_per_genome": per,
             "prescreen_ms_per_genome": round(pre_ms / ng, 2), "rescore_ms_per_genome": round(res_ms / ng, 2),
+            "viterbi_prescreen_ms_per_genome": round(vpre_ms / ng, 2),
             "launches_per_genome": int(statistics.median(launches)),
             "per_genome": {"final_pairs": round(pin[4] / ng, 1), "envelopes_on_device": round(pout[5] / ng, 1),
                            "regions_to_device": round(pin[6] / ng, 1), "regions_traced_on_device": round(pout[6] / ng, 1)},
@@ -570,7 +572,7 @@ def main():
     rps = reng.load_text(text, source="pfam_scale")
     rts = reng.targets_digital(seq, offs, lens)
     reng.search(rps, rts, cfg)  # warm-up
-    msv_ms, msv_cells, single_ms, pre = [], [], [], []
+    msv_ms, msv_cells, single_ms, pre, vpre, vit_ms = [], [], [], [], [], []
     for _ in range(2):
         flush_l2(torch, l2)
         torch.cuda.synchronize()
@@ -583,6 +585,8 @@ def main():
         msv_ms.append(rst["ms"][0])
         msv_cells.append(rst["cells"][0])
         pre.append(rst["prescreen"])
+        vpre.append(rst["vprescreen"])
+        vit_ms.append(rst["ms"][2])
     # stage GCUPS (cells entering a stage / its device time), single-block search
     stage_gcups = {k: round(rst["cells"][i] / (rst["ms"][i] / 1e3) / 1e9, 1) if rst["ms"][i] > 0 else None
                    for k, i in (("msv", 0), ("viterbi", 2), ("forward", 3), ("fwd_bwd_rows", 4))}
@@ -667,6 +671,12 @@ def main():
                  "prescreen_ms": round(pre_ms, 3), "rescore_ms": round(statistics.median([x["rescore_ms"] for x in pre]), 3),
                  "msv_stage_ms": round(statistics.median(msv_ms), 3),
                  "gcups": round(pre_cells / (pre_ms / 1e3) / 1e9, 1) if pre_ms > 0 else None}
+    # the packed Viterbi pre-screen in front of the exact Viterbi (stage 2)
+    vp_ms = statistics.median([x["ms"] for x in vpre])
+    vit_prescreen = {"pairs_in": vpre[-1]["pairs_in"], "pairs_passed": vpre[-1]["pairs_out"],
+                     "pass_fraction": vpre[-1]["pairs_out"] / max(1, vpre[-1]["pairs_in"]),
+                     "prescreen_ms": round(vp_ms, 3), "viterbi_stage_ms": round(statistics.median(vit_ms), 3),
+                     "gcups": round(vpre[-1]["cells"] / (vp_ms / 1e3) / 1e9, 1) if vp_ms > 0 else None}
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "msv_traffic.json")
     if os.path.exists(tfile):
@@ -694,6 +704,7 @@ def main():
                                 "note": f"{smem_bytes:.0f} B of emission score read from shared memory per DP cell; "
                                         "peak 128 B per clock per SM x 148 SMs x median sampled SM clock"},
             "msv_prescreen": prescreen,
+            "viterbi_prescreen": vit_prescreen,
             "stage_ms": {k: round(v / max(1, args.steps), 3) for k, v in zip(STAGES, stage_ms)},
             "stage_pairs_in": dict(zip(["msv", "bias", "viterbi", "forward", "rows", "host_domains"], stage_pairs or [])),
             "stage_gcups": stage_gcups, "stage_cells": stage_cells,

@@ -225,6 +225,12 @@ typedef struct {
    * of the pre-screen and of the exact rescoring */
   int64_t prescreen_pairs_in, prescreen_pairs_out;
   double prescreen_cells, prescreen_ms, rescore_ms;
+  /* the packed Viterbi pre-screen (part of stage 2): bias-filter survivors
+   * it bounded, those whose bound passed F2 (scored exactly; the exact
+   * Viterbi also takes the pairs of profiles it does not handle), its DP
+   * cells and device time */
+  int64_t vprescreen_pairs_in, vprescreen_pairs_out;
+  double vprescreen_cells, vprescreen_ms;
 } sx_search_stats;
 int sx_last_search_stats(const sx_engine* e, sx_search_stats* out);
 
@@ -263,9 +269,15 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
  *     the exact Forward score is bounded by (L+1)(2M + 6 VC + 64) 2^-24 nats,
  *     taken twice (VC = columns per lane of the profile's warp-chunked image);
  *     NaN for M > 2048.
- * Either output pointer may be NULL to skip that screen. */
+ *   vit_bound: the packed int16x2 Viterbi pre-screen's upper bound of the
+ *     f32 Viterbi score (nats; +inf when capped).  It is >= the viterbi score
+ *     of sx_score_pairs for every pair; NaN for empty targets and for
+ *     profiles the pre-screen does not handle (M > 512, profiles outside the
+ *     MSV pre-screen, match scores above +16 nats).
+ * Any output pointer may be NULL to skip that screen. */
 int sx_score_prescreens(sx_engine* e, const sx_profiles* p, const sx_targets* t, const int32_t* pair_profile,
-                        const int32_t* pair_target, size_t npairs, float* msv_bound, float* fwd_scan);
+                        const int32_t* pair_target, size_t npairs, float* msv_bound, float* fwd_scan,
+                        float* vit_bound);
 
 /* ---- adjoint ----------------------------------------------------------- */
 /* Gradient of each pair's Forward log score lnZ (multihit, target-length

@@ -162,6 +162,7 @@ const KernelTables& kernels() {
     fill_msv_tables(k);
     fill_msv16_tables(k);
     fill_vit_tables(k);
+    fill_vit16_tables(k);
     fill_vbin_tables(k);
     fill_env_tables(k);
     return k;
@@ -215,6 +216,14 @@ int choose_vit_shape(int m) {
 int vit_blocks(int num_sms, int shape, unsigned n) {
   const int g = kVitShapes[shape].g, per_sm = vit_ctas_per_sm(kVitShapes[shape]);
   return (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n * g + 255) / 256, (int64_t)num_sms * per_sm));
+}
+
+// Packed Viterbi pre-screen shape of a profile: the narrowest that covers M;
+// -1 when none does.
+int choose_vit16_shape(int m) {
+  for (int s = 0; s < kNumVit16Shapes; s++)
+    if (kVit16Shapes[s].g * kVit16Shapes[s].c >= m) return s;
+  return -1;
 }
 
 // Forward/Backward pass kernels run one warp per pair in one-warp CTAs, so a
@@ -430,6 +439,13 @@ struct Slot {
   DevBuf<int32_t> rlist;           // pre-screen survivors: target indices, rcap per profile of the block
   DevBuf<unsigned> rcount;         // survivors per profile of the block
   cudaEvent_t pre_done = nullptr;  // pre-screen finished (its time, for the stats)
+  // packed Viterbi pre-screen: the bias filter's survivors of pre-screened
+  // profiles, vcap per profile of the block, and the pre-screen's tiles
+  DevBuf<PairRec> vlist;
+  DevBuf<unsigned> vcount;
+  DevBuf<sxk::VitTile> vtiles;
+  DevBuf<double> vstats;           // cells bounded, cells passed, pairs passed
+  cudaEvent_t bias_done = nullptr, vpre_done = nullptr;
   // Forward/Backward row passes of the block's final pairs, in buffers of
   // their own: the engine thread queues them and moves on to the next block;
   // a host job waits for them, copies the rows out and releases the buffers.
@@ -452,6 +468,8 @@ struct Slot {
     lo.create(least, 5);
     for (auto& e : ev) CK(cudaEventCreate(&e));
     CK(cudaEventCreate(&pre_done));
+    CK(cudaEventCreate(&bias_done));
+    CK(cudaEventCreate(&vpre_done));
     CK(cudaEventCreate(&rows_t0));
     CK(cudaEventCreate(&rows_t1));
     CK(cudaStreamCreateWithFlags(&rows_copy, cudaStreamNonBlocking));
@@ -464,6 +482,8 @@ struct Slot {
       if (e) cudaEventDestroy(e);
     if (msv_done) cudaEventDestroy(msv_done);
     if (pre_done) cudaEventDestroy(pre_done);
+    if (bias_done) cudaEventDestroy(bias_done);
+    if (vpre_done) cudaEventDestroy(vpre_done);
     if (rows_busy) rows_busy->wait();
     if (rows_t0) cudaEventDestroy(rows_t0);
     if (rows_t1) cudaEventDestroy(rows_t1);
@@ -547,6 +567,7 @@ struct sx_profiles {
   DevBuf<float4> d_msv;
   DevBuf<uint2> d_qimg;  // quantized MSV images of the pre-screen (int16, 4 columns per uint2)
   DevBuf<float4> d_vit;  // Viterbi lane-group images
+  DevBuf<uint4> d_qvimg;  // quantized Viterbi images of the packed pre-screen
   DevBuf<float> d_vfb;
   DevBuf<double> d_bias;
 };
@@ -743,6 +764,73 @@ int pack_qimage(const ProfileHost& h, const DevProfile& d, uint2* out) {
   return emax;
 }
 
+// Quantized Viterbi image of the packed pre-screen (prescreen.cuh
+// vit16_kernel), in units of 2^-9 nat: every score rounded up after adding
+// 2^-12 nat; match scores clamped up to -8 nats, transitions clamped to
+// [-8 nats, 0] (t_bm to [-16 nats, 0]); -inf scores and columns past M take
+// the floor.  8 transition rows (each column's score in both int16 halves of
+// a word, 4 columns per uint4), then 25 match-score rows (4 columns per
+// uint2), lane-major like the f32 Viterbi image, at width G*C of the
+// profile's pre-screen shape.  Returns the largest rounded match score.
+int pack_qvimage(const ProfileHost& h, const DevProfile& d, uint4* out) {
+  const int m = h.m, G = kVit16Shapes[d.qv_shape].g, C = kVit16Shapes[d.qv_shape].c, NC4 = C / 4;
+  auto up = [](float v) { return std::ceil(((double)v + std::ldexp(1.0, -12)) * 512.0); };
+  int emax = sxk::kV16EFloor;
+  auto em = [&](int x, int k) -> int {
+    if (k > m) return sxk::kV16EFloor;
+    const float e = h.msc_row(x)[k];
+    if (!(e > -1e30f)) return sxk::kV16EFloor;
+    const int v = (int)std::max<double>(up(e), (double)sxk::kV16EFloor);
+    emax = std::max(emax, v);
+    return v;
+  };
+  auto tq = [&](float t, int floor) -> int {
+    if (!(t > -1e30f)) return floor;
+    return (int)std::max<double>(std::min<double>(up(t), 0.0), (double)floor);
+  };
+  const auto& t = h.t;
+  // transition row q of column k (the f32 Viterbi image's rows 25..32)
+  auto tr = [&](int q, int k) -> int {
+    if (k > m) return q == 3 ? sxk::kV16BmFloor : sxk::kV16TFloor;
+    switch (q) {
+      case 0: return tq(t[TMM][k - 1], sxk::kV16TFloor);
+      case 1: return tq(t[TIM][k - 1], sxk::kV16TFloor);
+      case 2: return tq(t[TDM][k - 1], sxk::kV16TFloor);
+      case 3: return tq(t[TBM][k], sxk::kV16BmFloor);
+      case 4: return k < m ? tq(t[TMI][k], sxk::kV16TFloor) : sxk::kV16TFloor;
+      case 5: return k < m ? tq(t[TII][k], sxk::kV16TFloor) : sxk::kV16TFloor;
+      case 6: return tq(t[TMD][k - 1], sxk::kV16TFloor);
+      default: return tq(t[TDD][k - 1], sxk::kV16TFloor);
+    }
+  };
+  auto dup = [](int v) { return ((uint32_t)v & 0xffffu) * 0x10001u; };
+  uint4* base = out + d.qv_off;
+  const size_t row4 = (size_t)NC4 * G;
+  for (int q = 0; q < 8; q++)
+    for (int j = 0; j < G; j++)
+      for (int c4 = 0; c4 < NC4; c4++) {
+        const int k = j * C + c4 * 4 + 1;
+        base[(q * NC4 + c4) * G + j] = make_uint4(dup(tr(q, k)), dup(tr(q, k + 1)), dup(tr(q, k + 2)), dup(tr(q, k + 3)));
+      }
+  uint2* es = reinterpret_cast<uint2*>(base + 8 * row4);
+  for (int x = 0; x < 25; x++)
+    for (int j = 0; j < G; j++)
+      for (int c4 = 0; c4 < NC4; c4++) {
+        int v[4];
+        for (int e = 0; e < 4; e++) v[e] = em(x, j * C + c4 * 4 + e + 1);
+        uint2 w;
+        w.x = (uint32_t)(v[0] & 0xffff) | ((uint32_t)(v[1] & 0xffff) << 16);
+        w.y = (uint32_t)(v[2] & 0xffff) | ((uint32_t)(v[3] & 0xffff) << 16);
+        es[((size_t)x * NC4 + c4) * G + j] = w;
+      }
+  return emax;
+}
+// uint4 entries of a quantized Viterbi image of shape s
+int64_t qvimage_size(int s) {
+  const int64_t row4 = (int64_t)(kVit16Shapes[s].c / 4) * kVit16Shapes[s].g;
+  return 8 * row4 + 25 * row4 / 2;
+}
+
 // Composition-bias filter table (src/hmmer/pipeline.rs:110-131): 54 doubles.
 void pack_bias(const ProfileHost& h, double* b) {
   const int m = h.m;
@@ -770,7 +858,7 @@ void pack_profiles(sx_profiles* P) {
   const size_t np = P->h.size();
   P->dp.resize(np);
   P->msv_shape.resize(np);
-  int64_t msv_total = 0, vfb_total = 0, vit_total = 0, q_total = 0;
+  int64_t msv_total = 0, vfb_total = 0, vit_total = 0, q_total = 0, qv_total = 0;
   for (size_t i = 0; i < np; i++) {
     const ProfileHost& h = P->h[i];
     DevProfile& d = P->dp[i];
@@ -784,6 +872,8 @@ void pack_profiles(sx_profiles* P) {
       d.vfb_off = vfb_total;
       d.vit_off = vit_total;
       d.q_off = -1;
+      d.qv_shape = -1;
+      d.qv_off = -1;
       continue;
     }
     const int s = shape_for(P->eng, 0, h.m);
@@ -805,12 +895,19 @@ void pack_profiles(sx_profiles* P) {
     if (d.vshape < 0) throw CudaError{SX_EINVAL, "profile '" + h.name + "' too long for the Viterbi shapes"};
     d.vit_off = vit_total;
     vit_total += 33LL * (kVitShapes[d.vshape].c / 4) * kVitShapes[d.vshape].g;
+    d.qv_shape = choose_vit16_shape(h.m);
+    d.qv_off = -1;
+    if (d.qv_shape >= 0) {
+      d.qv_off = qv_total;
+      qv_total += qvimage_size(d.qv_shape);
+    }
   }
   std::vector<float4> msv((size_t)msv_total);
   std::vector<float4> vit((size_t)std::max<int64_t>(vit_total, 1));
   std::vector<float> vfb((size_t)vfb_total);
   std::vector<double> bias(np * 54);
   std::vector<uint2> qimg((size_t)std::max<int64_t>(q_total, 1));
+  std::vector<uint4> qvimg((size_t)std::max<int64_t>(qv_total, 1));
   for (size_t i = 0; i < np; i++) {
     if (P->dp[i].vbin >= 0) {
       pack_images(P->h[i], P->dp[i], msv.data(), vit.data(), vfb.data());
@@ -819,6 +916,17 @@ void pack_profiles(sx_profiles* P) {
       const int emax = pack_qimage(P->h[i], P->dp[i], qimg.data());
       if (emax < 8192) P->dp[i].q_cap = 32767 - emax;
       else P->dp[i].q_off = -1;
+      // the Viterbi pre-screen takes the MSV pre-screen's profiles (whose
+      // bias-filter survivors fit the per-profile lists of the MSV rescoring)
+      // whose rounded match scores leave at least half of the int16 range
+      DevProfile& d = P->dp[i];
+      if (d.qv_shape >= 0 && d.q_off >= 0) {
+        const int vmax = pack_qvimage(P->h[i], d, qvimg.data());
+        if (vmax < 8192) d.qv_cap = 32767 - vmax;
+        else d.qv_shape = -1;
+      } else {
+        d.qv_shape = -1;
+      }
     }
     pack_bias(P->h[i], bias.data() + i * 54);
   }
@@ -852,6 +960,7 @@ void pack_profiles(sx_profiles* P) {
   P->d_prof.upload(P->dp.data(), np, s);
   P->d_msv.upload(msv.data(), msv.size(), s);
   P->d_qimg.upload(qimg.data(), qimg.size(), s);
+  P->d_qvimg.upload(qvimg.data(), qvimg.size(), s);
   P->d_vit.upload(vit.data(), vit.size(), s);
   P->d_vfb.upload(vfb.data(), vfb.size(), s);
   P->d_bias.upload(bias.data(), bias.size(), s);
@@ -1489,8 +1598,18 @@ void launch_rescore(sx_engine* E, Slot& S, Streams& X, const sx_profiles* P, con
              rcap, p0);
 }
 
+// Per-profile lists of the packed Viterbi pre-screen: with `list` set, the
+// bias filter hands the survivors of pre-screened profiles over in them.
+struct VitScreen {
+  PairRec* list = nullptr;
+  unsigned cap = 0;
+  unsigned* count = nullptr;
+  int p0 = 0;
+};
+
 // One filter stage over per-vbin lists: stage `si` reads lists[si] and writes lists[si+1].
-void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T, int si, const std::vector<unsigned>& nin) {
+void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T, int si, const std::vector<unsigned>& nin,
+                  const VitScreen& vs = VitScreen{}) {
   const auto& K = kernels();
   cudaStream_t s = S.hi.main;
   unsigned* cin = S.counts.p + si * kMaxBins;
@@ -1502,7 +1621,7 @@ void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets*
     dim3 grid((unsigned)std::min<int64_t>((mx + 255) / 256, (int64_t)E->num_sms * 8), kNumVbins);
     sxk::bias_kernel<<<grid, 256, 0, s>>>(S.lists[0].p, cin, S.bins[0].p, S.lists[1].p, S.bins[1].p, cout,
                                           S.overflow.p, P->d_bias.p, E->thr.p, T->d_res.p, T->d_off.p, T->d_len.p,
-                                          kSlackBits, nullptr, P->d_prof.p);
+                                          kSlackBits, nullptr, P->d_prof.p, vs.list, vs.cap, vs.count, vs.p0);
     E->stats.kernel_launches++;
   } else {
     if (si == 1) {
@@ -1539,6 +1658,45 @@ void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets*
     join_aux(S.hi);
   }
   CK(cudaGetLastError());
+}
+
+// Packed Viterbi pre-screen of a block's bias-filter survivors (profiles
+// `prof`, per-profile lists in `vs`): per profile `nsub` strided sub-tiles of
+// its list, larger M first, one launch per shape on the slot's high-priority
+// auxiliary streams; pairs whose bound passes F2 go to the Viterbi lists
+// (lists[2] of stage 1), S.vstats collects cells and passes.
+void launch_vprescreen(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T, const std::vector<int>& prof,
+                       const VitScreen& vs) {
+  const auto& K = kernels();
+  std::vector<std::vector<sxk::VitTile>> by_shape(kNumVit16Shapes);
+  const int nsub = std::max(2, std::min(32, (int)std::ceil(8.0 * E->num_sms / std::max<size_t>(1, prof.size()))));
+  std::vector<int> order(prof);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return P->h[a].m > P->h[b].m; });
+  for (int pi : order)
+    for (int q = 0; q < nsub; q++) by_shape[P->dp[pi].qv_shape].push_back({pi, q, nsub, 0});
+  std::vector<sxk::VitTile> all;
+  std::vector<size_t> start(kNumVit16Shapes + 1, 0);
+  for (int s = 0; s < kNumVit16Shapes; s++) {
+    start[s] = all.size();
+    all.insert(all.end(), by_shape[s].begin(), by_shape[s].end());
+  }
+  start[kNumVit16Shapes] = all.size();
+  if (all.empty()) return;
+  S.vtiles.upload(all.data(), all.size(), S.hi.main);
+  fork_aux(S.hi);
+  int lane = 0;
+  for (int s = kNumVit16Shapes - 1; s >= 0; s--) {  // widest first
+    if (start[s + 1] == start[s]) continue;
+    const int smem = vit16_smem(kVit16Shapes[s]);
+    CK(cudaFuncSetAttribute((const void*)K.vit16[s], cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    K.vit16[s]<<<(unsigned)(start[s + 1] - start[s]), 256, smem, S.hi.aux[lane++ % S.hi.naux]>>>(
+        S.vtiles.p + start[s], P->d_prof.p, E->thr.p, P->d_qvimg.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p,
+        vs.list, vs.cap, vs.count, vs.p0, S.lists[1].p, S.bins[1].p, S.counts.p + kMaxBins, S.overflow.p, kSlackBits,
+        nullptr, S.vstats.p);
+    E->stats.kernel_launches++;
+  }
+  CK(cudaGetLastError());
+  join_aux(S.hi);
 }
 
 double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
@@ -1992,6 +2150,7 @@ struct BlockRun {
   int attempt = 0;  // survivor-list sizing attempt; lists grow 4x per overflow
   std::vector<int> screened;  // profiles that go through the packed pre-screen
   unsigned rcap = 0;          // rescoring-list capacity per profile
+  std::vector<int> vscreened;  // profiles whose bias survivors go through the packed Viterbi pre-screen
   StageLists L[4];
   std::vector<double> pairs_in_bin, pairs_in_vs;
   double cells_total = 0;
@@ -2076,6 +2235,19 @@ void cascade_launch(sx_engine* E, Slot& S, const sx_profiles* P, const sx_target
       CK(cudaEventRecord(S.pre_done, s));
       launch_rescore(E, S, S.lo, P, T, R.screened, R.rcap, R.p0);
     }
+    // Viterbi pre-screen: every MSV-pre-screened profile with a quantized
+    // Viterbi image; its bias survivors (at most its rescoring list) go to
+    // per-profile lists of the same capacity
+    R.vscreened.clear();
+    for (int pi : R.screened)
+      if (P->dp[pi].qv_shape >= 0) R.vscreened.push_back(pi);
+    if (!R.vscreened.empty()) {
+      S.vlist.alloc((size_t)(R.p1 - R.p0) * R.rcap);
+      S.vcount.alloc((size_t)(R.p1 - R.p0));
+      S.vstats.alloc(3);
+      CK(cudaMemsetAsync(S.vcount.p, 0, sizeof(unsigned) * (R.p1 - R.p0), s));
+      CK(cudaMemsetAsync(S.vstats.p, 0, sizeof(double) * 3, s));
+    }
   }
   CK(cudaEventRecord(S.ev[1], s));
   CK(cudaEventRecord(S.msv_done, s));
@@ -2097,6 +2269,14 @@ bool cascade_finish(sx_engine* E, Slot& S, const sx_profiles* P, const sx_target
     std::vector<unsigned> nin(kMaxBins);
     for (int b = 0; b < kMaxBins; b++) nin[b] = std::min(cnt[si * kMaxBins + b], R.L[si].reg[b].cap);
     CK(cudaEventRecord(S.ev[2 + si], s));
+    if (si == 0 && !R.vscreened.empty()) {
+      const VitScreen vs{S.vlist.p, R.rcap, S.vcount.p, R.p0};
+      launch_stage(E, S, P, T, si, nin, vs);
+      CK(cudaEventRecord(S.bias_done, s));
+      launch_vprescreen(E, S, P, T, R.vscreened, vs);
+      CK(cudaEventRecord(S.vpre_done, s));
+      continue;
+    }
     launch_stage(E, S, P, T, si, nin);
     if (si >= 1) {  // cells entering Viterbi (si = 1) and the Forward pre-screen (si = 2), for the stats
       unsigned mx = 0;
@@ -2127,13 +2307,32 @@ bool cascade_finish(sx_engine* E, Slot& S, const sx_profiles* P, const sx_target
   for (int b = 0; b < kMaxBins; b++) pairs_all += R.pairs_in_bin[b];
   E->stats.pairs_in[0] += (int64_t)pairs_all;
   E->stats.cells[0] += R.cells_total;
+  // Viterbi pre-screen: its input are bias survivors, its passes part of
+  // the exact Viterbi's input
+  int64_t v_in = 0, v_pass = 0;
+  double v_stats[3] = {0, 0, 0};
+  if (!R.vscreened.empty()) {
+    std::vector<unsigned> vc((size_t)(R.p1 - R.p0));
+    CK(cudaMemcpyAsync(vc.data(), S.vcount.p, sizeof(unsigned) * vc.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(v_stats, S.vstats.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int pi : R.vscreened) v_in += std::min(vc[pi - R.p0], R.rcap);
+    v_pass = (int64_t)v_stats[2];
+    E->stats.vprescreen_pairs_in += v_in;
+    E->stats.vprescreen_pairs_out += v_pass;
+    E->stats.vprescreen_cells += v_stats[0];
+    E->stats.vprescreen_ms += elapsed_ms(S.bias_done, S.vpre_done);
+  }
   for (int si = 0; si < 4; si++) {
     int64_t c = 0;
     for (int b = 0; b < kMaxBins; b++) c += cnt[si * kMaxBins + b];
+    if (si == 1) c += v_in - v_pass;  // bias survivors: the pre-screen's input in place of its passes
     E->stats.pairs_out[si] += c;
     if (si < 3) E->stats.pairs_in[si + 1] += c;
   }
-  E->stats.cells[2] += scells[1];
+  // cells entering Viterbi: the exact kernel's input, with the pre-screen's
+  // passes replaced by all the pairs it bounded
+  E->stats.cells[2] += scells[1] - v_stats[1] + v_stats[0];
   E->stats.cells[3] += scells[2];
   E->stats.ms[0] += elapsed_ms(S.ev[0], S.ev[1]);
   if (!R.screened.empty()) {
@@ -2150,8 +2349,9 @@ bool cascade_finish(sx_engine* E, Slot& S, const sx_profiles* P, const sx_target
     E->stats.prescreen_ms += elapsed_ms(S.ev[0], S.pre_done);
     E->stats.rescore_ms += elapsed_ms(S.pre_done, S.ev[1]);
   }
-  E->stats.ms[1] += elapsed_ms(S.ev[2], S.ev[3]);
+  E->stats.ms[1] += elapsed_ms(S.ev[2], R.vscreened.empty() ? S.ev[3] : S.bias_done);
   E->stats.ms[2] += elapsed_ms(S.ev[3], S.ev[4]);
+  if (!R.vscreened.empty()) E->stats.ms[2] += elapsed_ms(S.bias_done, S.vpre_done);
   E->stats.ms[3] += elapsed_ms(S.ev[4], S.ev[5]);
   // gather stage-3 survivors
   std::vector<PairRec> surv;
@@ -3107,7 +3307,8 @@ int sx_score_pairs(sx_engine* e, const sx_profiles* p, const sx_targets* t, cons
 }
 
 int sx_score_prescreens(sx_engine* e, const sx_profiles* p, const sx_targets* t, const int32_t* pair_profile,
-                        const int32_t* pair_target, size_t npairs, float* msv_bound, float* fwd_scan) {
+                        const int32_t* pair_target, size_t npairs, float* msv_bound, float* fwd_scan,
+                        float* vit_bound) {
   if (!e || !p || !t || (npairs && (!pair_profile || !pair_target)))
     return fail(SX_EINVAL, "sx_score_prescreens: NULL argument");
   if (p->eng != e || t->eng != e) return fail(SX_EINVAL, "sx_score_prescreens: profiles/targets belong to another engine");
@@ -3120,6 +3321,7 @@ int sx_score_prescreens(sx_engine* e, const sx_profiles* p, const sx_targets* t,
   for (size_t i = 0; i < npairs; i++) {
     if (msv_bound) msv_bound[i] = NAN;
     if (fwd_scan) fwd_scan[i] = NAN;
+    if (vit_bound) vit_bound[i] = NAN;
   }
   if (!npairs) return SX_OK;
   try {
@@ -3175,6 +3377,49 @@ int sx_score_prescreens(sx_engine* e, const sx_profiles* p, const sx_targets* t,
           CK(cudaStreamSynchronize(s));  // the tile buffer is reused by the next shape
         }
         CK(cudaMemcpyAsync(msv_bound, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+      }
+    }
+    if (vit_bound) {
+      // pairs of Viterbi-pre-screened profiles, one list per profile; one
+      // launch per profile (its list at p0 = the profile, count at index 0)
+      std::vector<std::vector<int32_t>> byp(np);
+      for (size_t i = 0; i < npairs; i++)
+        if (p->dp[pair_profile[i]].qv_shape >= 0) byp[pair_profile[i]].push_back((int32_t)i);
+      std::vector<PairRec> recs;
+      std::vector<int64_t> seg;
+      std::vector<int> profs;
+      std::vector<unsigned> cnt;
+      for (size_t pi = 0; pi < np; pi++) {
+        if (byp[pi].empty()) continue;
+        profs.push_back((int)pi);
+        seg.push_back((int64_t)recs.size());
+        cnt.push_back((unsigned)byp[pi].size());
+        for (int32_t i : byp[pi]) recs.push_back({(int32_t)pi, pair_target[i], 0.f, 0.f, 0.f, 0.f, i, 0});
+      }
+      if (!recs.empty()) {
+        Slot& S = e->sl[0];
+        S.vlist.upload(recs.data(), recs.size(), s);
+        S.vcount.upload(cnt.data(), cnt.size(), s);
+        constexpr int kSub = 8;
+        std::vector<sxk::VitTile> tiles;
+        for (int pi : profs)
+          for (int q = 0; q < kSub; q++) tiles.push_back({pi, q, kSub, 0});
+        S.vtiles.upload(tiles.data(), tiles.size(), s);
+        e->scores.alloc(npairs);
+        std::vector<float> nanv(npairs, NAN);
+        CK(cudaMemcpyAsync(e->scores.p, nanv.data(), sizeof(float) * npairs, cudaMemcpyHostToDevice, s));
+        for (size_t q = 0; q < profs.size(); q++) {
+          const int sh = p->dp[profs[q]].qv_shape;
+          const int smem = vit16_smem(kVit16Shapes[sh]);
+          CK(cudaFuncSetAttribute((const void*)K.vit16[sh], cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+          K.vit16[sh]<<<kSub, 256, smem, s>>>(S.vtiles.p + q * kSub, p->d_prof.p, e->thr.p, p->d_qvimg.p, t->d_res.p,
+                                             t->d_off.p, t->d_len.p, t->d_xsc.p, S.vlist.p + seg[q], cnt[q],
+                                             S.vcount.p + q, profs[q], nullptr, nullptr, nullptr, e->overflow.p,
+                                             kSlackBits, e->scores.p, nullptr);
+        }
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(vit_bound, e->scores.p, sizeof(float) * npairs, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
       }
     }

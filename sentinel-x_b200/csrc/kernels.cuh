@@ -20,7 +20,7 @@ constexpr float kLn2 = 0.693147182464599609375f;
 constexpr unsigned kFull = 0xffffffffu;
 
 // ---- device records ------------------------------------------------------
-struct DevProfile {  // 72 bytes
+struct DevProfile {  // 88 bytes
   int32_t m;
   int32_t vc;        // columns per lane in the warp-chunked layout (32 lanes)
   int32_t vbin;      // survivor-list bin of vc
@@ -34,7 +34,10 @@ struct DevProfile {  // 72 bytes
   int64_t vit_off;   // float4 offset of the Viterbi image (33 rows, lane-major for that shape)
   int64_t q_off;     // uint2 offset of the quantized MSV image; -1: the profile is not pre-screened
   int32_t q_tbm;     // msv_tbm rounded up, units of 2^-20 nat (pre-screen entry constant)
-  int32_t pad1;
+  int32_t qv_shape;  // packed Viterbi pre-screen shape; -1: the profile is not pre-screened
+  int64_t qv_off;    // uint4 offset of its quantized Viterbi image
+  int32_t qv_cap;    // its row maxima above this (int16 units) pass at once
+  int32_t pad2;
 };
 struct Thresholds {  // per profile, per search: pass iff statistic >= threshold (bits)
   float s1, s2, s3;
@@ -285,6 +288,9 @@ __global__ void __launch_bounds__(256, 2) msv_kernel(const MsvTile* __restrict__
 // pair, in f64 with the device log.  Decision on the F1 threshold with slack;
 // the host re-checks survivors with the exact libm value.
 // btab per profile: eo0[25], eo1[25], t00, t01, t10, t11  (54 doubles)
+// With `vlist`, the survivors of profiles that have a packed Viterbi
+// pre-screen image go to their profile's list (region (p - p0) * vcap, count
+// vcount[p - p0]) instead of the Viterbi lists.
 // ===========================================================================
 static __global__ void __launch_bounds__(256) bias_kernel(const PairRec* __restrict__ in, const unsigned* __restrict__ in_counts,
                                                    const BinRegion* __restrict__ in_bins, PairRec* __restrict__ out,
@@ -293,7 +299,9 @@ static __global__ void __launch_bounds__(256) bias_kernel(const PairRec* __restr
                                                    const Thresholds* __restrict__ thr, const uint8_t* __restrict__ res,
                                                    const int64_t* __restrict__ toff, const int32_t* __restrict__ tlen,
                                                    float slack, float* __restrict__ score_out,
-                                                   const DevProfile* __restrict__ profs) {
+                                                   const DevProfile* __restrict__ profs,
+                                                   PairRec* __restrict__ vlist = nullptr, unsigned vcap = 0,
+                                                   unsigned* __restrict__ vcount = nullptr, int p0 = 0) {
   const int bin = blockIdx.y;
   const unsigned n = min(in_counts[bin], in_bins[bin].cap);
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -327,7 +335,15 @@ static __global__ void __launch_bounds__(256) bias_kernel(const PairRec* __restr
       score_out[r.slot] = fsc;
       continue;
     }
-    if (bits_stat(r.usc, fsc) >= thr[r.p].s1 - slack) push_pair(r, profs[r.p].vshape, out, out_bins, out_counts, overflow);
+    if (bits_stat(r.usc, fsc) >= thr[r.p].s1 - slack) {
+      if (vlist && profs[r.p].qv_shape >= 0) {
+        const unsigned pos = atomicAdd(&vcount[r.p - p0], 1u);
+        if (pos < vcap) vlist[(int64_t)(r.p - p0) * vcap + pos] = r;
+        else atomicOr(overflow, 1u);
+      } else {
+        push_pair(r, profs[r.p].vshape, out, out_bins, out_counts, overflow);
+      }
+    }
   }
 }
 

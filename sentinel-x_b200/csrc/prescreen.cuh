@@ -255,3 +255,342 @@ __global__ void __launch_bounds__(256, 2) msv16_kernel(
 }
 
 }  // namespace sxk
+
+namespace sxk {
+
+// ---------------------------------------------------------------------------
+// Packed-integer Viterbi pre-screen: an upper bound of the reference's f32
+// Viterbi score (src/hmmer/dp.rs:152-189) for two targets of one profile at
+// once, in int16x2 lanes (target a in the low half, b in the high half).
+//
+// Why: the exact lane-group kernel (viterbi_g_kernel) is bound by the
+// latency of each row's sequential parts -- the D chain, the carry vote, the
+// row-maximum butterfly, the special states -- and by the per-row control
+// around them, which a lane group pays once per pair.  Here one pass of all
+// of that serves two pairs: every 32-bit word holds the same column of two
+// DP rows, one max.s16x2 / add.s16x2 updates both, and the carry vote, the
+// butterfly and the loop control are shared.
+//
+// Exactness.  As for the MSV pre-screen, the bound never decides a pair: a
+// pair passes when its bound passes F2 (with the exact kernel's slack), and
+// every passing pair is rescored by viterbi_g_kernel, so the survivors of
+// the stage are exactly the reference's.  The bound holds by construction:
+//   * cells are integers in units of q = 2^-9 nat.  Match scores are rounded
+//     up after adding 2^-12 nat (more than the f32 rounding of one addition
+//     for |value| < 4096 nats) and clamped up to -8 nats; transition scores
+//     the same way, clamped up to -8 nats (t_bm: -16 nats) and down to 0 --
+//     a transition t <= 0 never raises a value (fl(a + t) <= a), so 0 bounds
+//     any t in [-2^-12, 0]; -inf scores become the floor.  Integer max-plus
+//     over rounded-up scores is >= the real-valued recurrence, which is >=
+//     the f32 recurrence minus its rounding; by induction every integer cell
+//     is >= the f32 cell (max is exact and monotone; raising an input only
+//     raises the result).  The insert rows ignore the '*' residue's
+//     insert-state cut (dp.rs:172), which only raises I;
+//   * the row maximum is taken over M alone: with every transition <= 0,
+//     D[k] <= max over k' < k of M[k'] in f32 and in the integers alike;
+//   * the specials are int32 in units of 2^-20 nat with every constant
+//     rounded up after adding 2^-17 nat, as in the MSV pre-screen;
+//   * the final bound (xJ + tmove at row L, rounded up to f32) goes through
+//     the exact kernel's f32 bit statistic, which is monotone.
+// int16 range: the floors keep every sum >= -28672 (B + t_bm >= -12 nats so
+// M >= -32 nats, D, I >= -40 nats, pre >= -48 nats, plus one more
+// transition); every value is <= the previous rows' maximum plus the largest
+// match score, so a row maximum above the profile's cap (32767 minus that
+// score) marks the pair as passing before anything can wrap (sticky).
+// Columns past M carry the floor scores; the profile's quantized image has
+// the kernel's width G*C and the CPU model follows the same columns.
+// ---------------------------------------------------------------------------
+constexpr int kV16TFloor = -4096;    // -8 nats: lowest transition score (t_bm excepted)
+constexpr int kV16BmFloor = -8192;   // -16 nats: lowest t_bm
+constexpr int kV16EFloor = -4096;    // -8 nats: lowest match score, and columns past M
+constexpr int kV16BFloor = -4096;    // -8 nats: lowest B state
+constexpr unsigned kV16Init2 = 0xc000c000u;  // (-16384, -16384): -inf before row 1 / left of column 1
+constexpr unsigned kV16Low2 = 0xa000a000u;   // (-24576, -24576): provisional D carry into a lane
+
+// One profile x every nsub-th entry (from sub) of its Viterbi pre-screen list.
+struct VitTile {
+  int32_t p, sub, nsub, pad;
+};
+
+// int16x2 helpers: replace one half of a word by the same half of v.
+__device__ __forceinline__ unsigned set_half(unsigned w, int h, unsigned v) {
+  return h ? __byte_perm(w, v, 0x7610) : __byte_perm(w, v, 0x3254);
+}
+
+// Bound of pairs of one profile (tile.p) against the targets of its list
+// (region (p - p0) * vcap of `vlist`, vcount[p - p0] entries).  The profile's
+// quantized image (qv_off, uint4 units): 8 transition rows of W/4 uint4 (each
+// column's score in both halves: t_mm t_im t_dm at k-1, t_bm t_mi t_ii at k,
+// t_md t_dd at k-1), then 25 match-score rows of W/4 uint2 (4 columns of
+// int16), both in the lane-major chunk layout of the f32 Viterbi image.
+// Per pair: with `score_out`, the bound (f32 nats; +inf when capped, NaN for
+// an empty target) goes to score_out[slot]; otherwise a pair whose bound
+// passes F2 is appended to the exact Viterbi's list (bin vshape).  stats[0..2]
+// accumulate the DP cells bounded, the cells of the passing pairs and the
+// passing pairs.
+template <int G, int C>
+__global__ void __launch_bounds__(256, (C <= 8 ? 2 : 1)) vit16_kernel(
+    const VitTile* __restrict__ tiles, const DevProfile* __restrict__ profs, const Thresholds* __restrict__ thr,
+    const uint4* __restrict__ qvimg, const uint8_t* __restrict__ res, const int64_t* __restrict__ toff,
+    const int32_t* __restrict__ tlen, const float4* __restrict__ xsc, const PairRec* __restrict__ vlist,
+    unsigned vcap, const unsigned* __restrict__ vcount, int p0, PairRec* __restrict__ out,
+    const BinRegion* __restrict__ out_bins, unsigned* __restrict__ out_counts, unsigned* __restrict__ overflow,
+    float slack, float* __restrict__ score_out, double* __restrict__ stats) {
+  static_assert(C % 4 == 0 && (G & (G - 1)) == 0 && G <= 32, "bad packed Viterbi shape");
+  constexpr int NC4 = C / 4;
+  constexpr int ROW4 = NC4 * G;  // uint4 per transition row, uint2 per score row
+  static_assert(ROW4 % 2 == 0, "score rows must fill whole uint4");
+  constexpr int NIMG4 = 8 * ROW4 + 25 * ROW4 / 2;
+  extern __shared__ uint4 sm_v[];
+  __shared__ unsigned s_next;
+  const VitTile tile = tiles[blockIdx.x];
+  const DevProfile P = profs[tile.p];
+  {
+    const uint4* src = qvimg + P.qv_off;
+    for (int q = threadIdx.x; q < NIMG4; q += blockDim.x) sm_v[q] = src[q];
+  }
+  if (threadIdx.x == 0) s_next = 0;
+  __syncthreads();
+  const uint4* Ts = sm_v;
+  const uint2* Es = reinterpret_cast<const uint2*>(sm_v + 8 * ROW4);
+
+  const int lane = threadIdx.x & 31;
+  const int j = lane & (G - 1);
+  const int gl = lane - j;
+  const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << gl);
+  const int pl = tile.p - p0;
+  const unsigned n = min(vcount[pl], vcap);
+  const PairRec* lst = vlist + (int64_t)pl * vcap;
+  const int cap = P.qv_cap;
+  const float s2 = thr[tile.p].s2;
+  const int nln2 = (int)ceilf(-0.693147182464599609375f * 1048576.0f) + kQ32Rho;
+  const uint4* tr = Ts + j;
+  auto T = [&](int q, int c4) -> uint4 { return tr[(q * NC4 + c4) * G]; };
+  auto pick = [](const uint4& v, int e) -> unsigned { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; };
+
+  unsigned mp[C], ip[C], dp[C], pre[C];
+#pragma unroll
+  for (int c = 0; c < C; c++) mp[c] = ip[c] = dp[c] = pre[c] = kV16Init2;
+  unsigned bw = kV16Init2;   // B of both halves for the row being computed
+  unsigned dpl = kV16Init2;  // left lane's D at its last column, previous row
+  // per half: pair state
+  int L[2] = {0, 0}, row[2] = {0, 0}, boff[2] = {0, 0}, idx[2] = {0, 0};
+  int xn[2] = {0, 0}, xj[2] = {kQ32Neg, kQ32Neg}, fin[2] = {kQ32Neg, kQ32Neg}, tl[2] = {0, 0}, tm[2] = {0, 0};
+  bool act[2] = {false, false}, big[2] = {false, false}, dn[2] = {false, false};
+  const uint8_t* seq[2] = {res, res};
+  uint4 rc[2], rn[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) rc[h] = rn[h] = make_uint4(0x18181818u, 0x18181818u, 0x18181818u, 0x18181818u);
+  double cells_in = 0.0, cells_pass = 0.0, npass = 0.0;
+
+  for (;;) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (!dn[h] && row[h] >= L[h]) {  // group-uniform: finish this half's pair, take the next one
+        if (act[h] && j == 0) {
+          const PairRec r = lst[idx[h]];
+          const float ub = L[h] == 0 ? __int_as_float(0x7fc00000)
+                           : big[h]  ? __int_as_float(0x7f800000)
+                                     : __fmul_rn(__int2float_ru(fin[h]), 9.5367431640625e-7f);
+          if (score_out) {
+            score_out[r.slot] = ub;
+          } else if (L[h] > 0) {
+            const double cells = (double)P.m * (double)L[h];
+            cells_in += cells;
+            if (big[h] || bits_stat(ub, r.filtersc) >= s2 - slack) {
+              push_pair(r, P.vshape, out, out_bins, out_counts, overflow);
+              cells_pass += cells;
+              npass += 1.0;
+            }
+          }
+        }
+        unsigned k = 0;
+        if (j == 0) k = atomicAdd(&s_next, 1u);
+        k = __shfl_sync(gmask, k, gl);
+        const unsigned e = (unsigned)tile.sub + k * (unsigned)tile.nsub;
+        if (k < n && e < n) {
+          idx[h] = (int)e;
+          const int t = lst[e].t;
+          L[h] = tlen[t];
+          seq[h] = res + toff[t];
+          const float4 xs = xsc[t];
+          tl[h] = q32_up(xs.x);
+          tm[h] = q32_up(xs.y);
+          xn[h] = 0;
+          xj[h] = kQ32Neg;
+          fin[h] = kQ32Neg;
+          big[h] = false;
+          row[h] = 0;
+          boff[h] = 0;
+          rc[h] = __ldg(reinterpret_cast<const uint4*>(seq[h]));
+          rn[h] = __ldg(reinterpret_cast<const uint4*>(seq[h] + 16));
+          act[h] = true;
+#pragma unroll
+          for (int c = 0; c < C; c++) {
+            mp[c] = set_half(mp[c], h, kV16Init2);
+            ip[c] = set_half(ip[c], h, kV16Init2);
+            dp[c] = set_half(dp[c], h, kV16Init2);
+            pre[c] = set_half(pre[c], h, kV16Init2);
+          }
+          dpl = set_half(dpl, h, kV16Init2);
+          // B of row 1: xB = tmove
+          const int b16 = max((tm[h] + 2047) >> (kQ32Shift - kQ16Shift), kV16BFloor);
+          bw = set_half(bw, h, ((unsigned)b16 & 0xffffu) * 0x10001u);
+        } else {
+          act[h] = false;
+          dn[h] = true;
+          L[h] = 0;
+        }
+      }
+    }
+    if (__all_sync(kFull, dn[0] && dn[1])) break;
+
+    // this row's residue of each half ('*' past the end and for idle halves)
+    int x[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int q = row[h] - boff[h];
+      const uint32_t w = (q >> 2) == 0 ? rc[h].x : (q >> 2) == 1 ? rc[h].y : (q >> 2) == 2 ? rc[h].z : rc[h].w;
+      x[h] = (act[h] && row[h] < L[h]) ? (int)((w >> (8 * (q & 3))) & 0xffu) : 24;
+    }
+    // match scores of both halves, interleaved into words
+    unsigned ew[C];
+    {
+      const uint2* ea = Es + x[0] * ROW4 + j;
+      const uint2* eb = Es + x[1] * ROW4 + j;
+#pragma unroll
+      for (int c4 = 0; c4 < NC4; c4++) {
+        const uint2 a = ea[c4 * G], b = eb[c4 * G];
+        ew[4 * c4 + 0] = __byte_perm(a.x, b.x, 0x5410);
+        ew[4 * c4 + 1] = __byte_perm(a.x, b.x, 0x7632);
+        ew[4 * c4 + 2] = __byte_perm(a.y, b.y, 0x5410);
+        ew[4 * c4 + 3] = __byte_perm(a.y, b.y, 0x7632);
+      }
+    }
+    // ---- M: max(pre, D[k-1] + t_dm, B + t_bm) + msc (dp.rs:167-169) ----
+#pragma unroll
+    for (int c4 = 0; c4 < NC4; c4++) {
+      const uint4 tdm = T(2, c4), tbm = T(3, c4);
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int c = 4 * c4 + e;
+        const unsigned dpv = c ? dp[c - 1] : dpl;
+        mp[c] = add2s16(max2s16(max2s16(pre[c], add2s16(dpv, pick(tdm, e))), add2s16(bw, pick(tbm, e))), ew[c]);
+      }
+    }
+    // ---- D chain (ascending; provisional carry into lanes other than the
+    // first), then the next row's pre and I (descending, in place) ----
+    const unsigned mcl0 = __shfl_up_sync(kFull, mp[C - 1], 1, G);
+    const unsigned ipl0 = __shfl_up_sync(kFull, ip[C - 1], 1, G);
+    const unsigned mcl = j ? mcl0 : kV16Init2, ipl = j ? ipl0 : kV16Init2;
+    {
+      unsigned d = j ? kV16Low2 : kV16Init2;
+#pragma unroll
+      for (int c4 = 0; c4 < NC4; c4++) {
+        const uint4 tmd = T(6, c4), tdd = T(7, c4);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int c = 4 * c4 + e;
+          const unsigned mcv = c ? mp[c - 1] : mcl;
+          d = max2s16(add2s16(mcv, pick(tmd, e)), add2s16(d, pick(tdd, e)));
+          dp[c] = d;
+        }
+      }
+    }
+#pragma unroll
+    for (int c4 = NC4 - 1; c4 >= 0; c4--) {
+      const uint4 tmm = T(0, c4), tim = T(1, c4), tmi = T(4, c4), tii = T(5, c4);
+#pragma unroll
+      for (int e = 3; e >= 0; e--) {
+        const int c = 4 * c4 + e;
+        const unsigned mpv = c ? mp[c - 1] : mcl, ipv = c ? ip[c - 1] : ipl;
+        pre[c] = max2s16(add2s16(mpv, pick(tmm, e)), add2s16(ipv, pick(tim, e)));
+        ip[c] = max2s16(add2s16(mp[c], pick(tmi, e)), add2s16(ip[c], pick(tii, e)));
+      }
+    }
+    // ---- carries across the group's lanes until nothing changes (exact:
+    // max-plus is monotone and the provisional carry is below every D) ----
+    bool settled = false;
+    for (int it = 0; it < G; it++) {
+      const unsigned c0 = __shfl_up_sync(kFull, dp[C - 1], 1, G);
+      unsigned cin = j ? c0 : kV16Init2;
+      const unsigned tdd0 = T(7, 0).x;
+      const bool need = max2s16(add2s16(cin, tdd0), dp[0]) != dp[0];
+      if (!__any_sync(kFull, need)) {
+        dpl = cin;
+        settled = true;
+        break;
+      }
+      bool go = true;
+#pragma unroll
+      for (int c4 = 0; c4 < NC4; c4++) {
+        if (go) {
+          const uint4 tdd = T(7, c4);
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const int c = 4 * c4 + e;
+            if (go) {
+              const unsigned nd = max2s16(dp[c], add2s16(cin, pick(tdd, e)));
+              if (nd == dp[c]) {
+                go = false;
+              } else {
+                dp[c] = nd;
+                cin = nd;
+              }
+            }
+          }
+        }
+      }
+    }
+    if (!settled) {
+      const unsigned d0 = __shfl_up_sync(kFull, dp[C - 1], 1, G);
+      dpl = j ? d0 : kV16Init2;
+    }
+    // ---- row maximum over M (D never exceeds it), per half ----
+    unsigned tv[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) tv[c] = mp[c];
+#pragma unroll
+    for (int span = 1; span < C; span <<= 1)
+#pragma unroll
+      for (int c = 0; c + span < C; c += 2 * span) tv[c] = max2s16(tv[c], tv[c + span]);
+    unsigned xe = tv[0];
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1) xe = max2s16(xe, __shfl_xor_sync(kFull, xe, o, G));
+    // ---- special states per half (xC == xJ, as in the exact kernel) ----
+    int b16[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int eh = h ? ((int)xe >> 16) : (int)(short)(xe & 0xffffu);
+      big[h] |= eh > cap;
+      xj[h] = max(xj[h] + tl[h], eh * 2048 + nln2);
+      xn[h] += tl[h];
+      const int xb = max(xn[h], xj[h]) + tm[h];
+      b16[h] = max((xb + 2047) >> (kQ32Shift - kQ16Shift), kV16BFloor);
+      row[h]++;
+      if (row[h] == L[h]) fin[h] = xj[h] + tm[h];
+      if (row[h] - boff[h] == 16) {
+        boff[h] += 16;
+        rc[h] = rn[h];
+        if (act[h]) rn[h] = __ldg(reinterpret_cast<const uint4*>(seq[h] + boff[h] + 16));
+      }
+    }
+    bw = __byte_perm((unsigned)b16[0], (unsigned)b16[1], 0x5410);
+  }
+  // stats: one atomic per warp
+  if (stats) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      cells_in += __shfl_xor_sync(kFull, cells_in, o);
+      cells_pass += __shfl_xor_sync(kFull, cells_pass, o);
+      npass += __shfl_xor_sync(kFull, npass, o);
+    }
+    if (lane == 0 && cells_in != 0.0) {
+      atomicAdd(stats + 0, cells_in);
+      atomicAdd(stats + 1, cells_pass);
+      atomicAdd(stats + 2, npass);
+    }
+  }
+}
+
+}  // namespace sxk

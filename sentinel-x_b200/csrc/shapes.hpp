@@ -1,7 +1,7 @@
 // Kernel shapes compiled into the library and the per-shape launch tables.
 //
 // The template instantiations live in their own translation units
-// (k_msv.cu, k_vit.cu, k_vbin.cu, k_env.cu) so the library builds in
+// (k_msv.cu, k_msv16.cu, k_vit.cu, k_vit16.cu, k_vbin.cu, k_env.cu) so the library builds in
 // parallel; engine.cu launches them through the function-pointer tables
 // filled here.
 #pragma once
@@ -54,6 +54,18 @@ constexpr int kNumVitShapes = sizeof(kVitShapes) / sizeof(kVitShapes[0]);
 constexpr int kMaxBins = 32;  // survivor lists per stage (vbins or Viterbi shapes)
 static_assert(kNumVitShapes <= kMaxBins, "too many Viterbi shapes");
 
+// Packed Viterbi pre-screen shapes (prescreen.cuh vit16_kernel): G lanes per
+// pair of targets, C columns per lane; a profile takes the narrowest that
+// covers M, profiles wider than the last one are not pre-screened.
+struct Vit16Shape {
+  int g, c;
+};
+constexpr Vit16Shape kVit16Shapes[] = {{4, 8}, {8, 8}, {16, 8}, {32, 8}, {32, 16}};
+constexpr int kNumVit16Shapes = sizeof(kVit16Shapes) / sizeof(kVit16Shapes[0]);
+// dynamic shared memory of one tile: 8 transition rows of 4 bytes per column
+// and 25 score rows of 2 bytes per column
+constexpr int vit16_smem(const Vit16Shape& v) { return 82 * v.g * v.c; }
+
 // Warp-chunked column counts (columns per lane, 32 lanes per pair).
 constexpr int kVcBins[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64};
 constexpr int kNumVbins = sizeof(kVcBins) / sizeof(kVcBins[0]);
@@ -64,6 +76,9 @@ typedef void (*MsvFn)(const MsvTile*, const DevProfile*, const Thresholds*, cons
 typedef void (*Msv16Fn)(const sxk::PackedTile*, const DevProfile*, const Thresholds*, const uint2*, const uint8_t*,
                         const int64_t*, const int32_t*, const float4*, const int32_t*, int32_t*, unsigned, unsigned*,
                         int, unsigned*, float*, const int32_t*, int64_t);
+typedef void (*Vit16Fn)(const sxk::VitTile*, const DevProfile*, const Thresholds*, const uint4*, const uint8_t*,
+                        const int64_t*, const int32_t*, const float4*, const PairRec*, unsigned, const unsigned*, int,
+                        PairRec*, const BinRegion*, unsigned*, unsigned*, float, float*, double*);
 typedef void (*VitFn)(const PairRec*, const unsigned*, const BinRegion*, int, PairRec*, const BinRegion*, unsigned*,
                       unsigned*, const DevProfile*, const Thresholds*, const float*, const uint8_t*, const int64_t*,
                       const int32_t*, const float4*, float, float*);
@@ -97,12 +112,14 @@ struct KernelTables {
   AdjFFn adjf[kNumVbins];
   AdjBFn adjb[kNumVbins];
   VitGFn vitg[kNumVitShapes];
+  Vit16Fn vit16[kNumVit16Shapes];  // the packed Viterbi pre-screen
 };
 
 // Filled by the kernel translation units.
 void fill_msv_tables(KernelTables& t);
 void fill_msv16_tables(KernelTables& t);
 void fill_vit_tables(KernelTables& t);
+void fill_vit16_tables(KernelTables& t);
 void fill_vbin_tables(KernelTables& t);
 void fill_env_tables(KernelTables& t);
 

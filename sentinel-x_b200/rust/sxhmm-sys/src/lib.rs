@@ -168,6 +168,10 @@ pub mod ffi {
         pub prescreen_cells: f64,
         pub prescreen_ms: f64,
         pub rescore_ms: f64,
+        pub vprescreen_pairs_in: i64,
+        pub vprescreen_pairs_out: i64,
+        pub vprescreen_cells: f64,
+        pub vprescreen_ms: f64,
     }
 
     extern "C" {
@@ -214,7 +218,7 @@ pub mod ffi {
                               viterbi: *mut f32, forward: *mut f32, backward: *mut f32, bias: *mut f32) -> c_int;
         pub fn sx_score_prescreens(e: *mut sx_engine, p: *const sx_profiles, t: *const sx_targets,
                                    pair_profile: *const i32, pair_target: *const i32, npairs: usize,
-                                   msv_bound: *mut f32, fwd_scan: *mut f32) -> c_int;
+                                   msv_bound: *mut f32, fwd_scan: *mut f32, vit_bound: *mut f32) -> c_int;
         pub fn sx_posterior_grad(e: *mut sx_engine, p: *const sx_profiles, t: *const sx_targets,
                                  pair_profile: *const i32, pair_target: *const i32, npairs: usize, m: i32,
                                  d_msc: *mut f32, d_isc: *mut f32, d_trans: *mut f32, lnz: *mut f64) -> c_int;

@@ -63,7 +63,8 @@ class SxSearchStats(C.Structure):
     _fields_ = [("pairs_in", C.c_int64 * 8), ("pairs_out", C.c_int64 * 8), ("cells", C.c_double * 8),
                 ("ms", C.c_double * 8), ("kernel_launches", C.c_int64), ("prescreen_pairs_in", C.c_int64),
                 ("prescreen_pairs_out", C.c_int64), ("prescreen_cells", C.c_double), ("prescreen_ms", C.c_double),
-                ("rescore_ms", C.c_double)]
+                ("rescore_ms", C.c_double), ("vprescreen_pairs_in", C.c_int64),
+                ("vprescreen_pairs_out", C.c_int64), ("vprescreen_cells", C.c_double), ("vprescreen_ms", C.c_double)]
 
 
 _i32p = C.POINTER(C.c_int32)
@@ -105,7 +106,7 @@ SIGNATURES = {
     "sx_score_pairs": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, _fp, _fp, _fp, _fp, _fp]),
     "sx_posterior_grad": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, C.c_int32, _fp, _fp, _fp, _dp]),
     "sx_score_viterbi_static": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, _fp]),
-    "sx_score_prescreens": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, _fp, _fp]),
+    "sx_score_prescreens": (C.c_int, [_P, _P, _P, _i32p, _i32p, C.c_size_t, _fp, _fp, _fp]),
 }
 
 
@@ -248,7 +249,9 @@ class Engine:
         return {"pairs_in": list(s.pairs_in), "pairs_out": list(s.pairs_out), "cells": list(s.cells),
                 "ms": list(s.ms), "kernel_launches": s.kernel_launches,
                 "prescreen": {"pairs_in": s.prescreen_pairs_in, "pairs_out": s.prescreen_pairs_out,
-                              "cells": s.prescreen_cells, "ms": s.prescreen_ms, "rescore_ms": s.rescore_ms}}
+                              "cells": s.prescreen_cells, "ms": s.prescreen_ms, "rescore_ms": s.rescore_ms},
+                "vprescreen": {"pairs_in": s.vprescreen_pairs_in, "pairs_out": s.vprescreen_pairs_out,
+                               "cells": s.vprescreen_cells, "ms": s.vprescreen_ms}}
 
     def score_pairs(self, profiles, targets, pp, pt, stages=("msv", "viterbi", "forward", "backward", "bias")):
         pp = np.ascontiguousarray(pp, dtype=np.int32)
@@ -263,17 +266,19 @@ class Engine:
         return {s: v[:n] for s, v in out.items()}
 
     def score_prescreens(self, profiles, targets, pp, pt):
-        """The two conservative screens for explicit pairs (sx_score_prescreens):
+        """The conservative screens for explicit pairs (sx_score_prescreens):
         {"msv_bound": packed MSV pre-screen bound, "fwd_scan": F3 pre-screen
-        Forward score}, float32 arrays (nats)."""
+        Forward score, "vit_bound": packed Viterbi pre-screen bound}, float32
+        arrays (nats)."""
         pp = np.ascontiguousarray(pp, dtype=np.int32)
         pt = np.ascontiguousarray(pt, dtype=np.int32)
         n = len(pp)
         mb = np.full(max(n, 1), np.nan, np.float32)
         fs = np.full(max(n, 1), np.nan, np.float32)
+        vb = np.full(max(n, 1), np.nan, np.float32)
         _check(_lib.sx_score_prescreens(self.h, profiles.h, targets.h, _ptr(pp, C.c_int32), _ptr(pt, C.c_int32), n,
-                                        _ptr(mb, C.c_float), _ptr(fs, C.c_float)))
-        return {"msv_bound": mb[:n], "fwd_scan": fs[:n]}
+                                        _ptr(mb, C.c_float), _ptr(fs, C.c_float), _ptr(vb, C.c_float)))
+        return {"msv_bound": mb[:n], "fwd_scan": fs[:n], "vit_bound": vb[:n]}
 
     def posterior_grad(self, profiles, targets, pp, pt, m, out=None):
         """lnZ and its gradients for each pair (sx_posterior_grad).  `out`:

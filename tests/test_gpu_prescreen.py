@@ -5,6 +5,10 @@
   never below the reference's f32 MSV score (src/hmmer/dp.rs:92-145; the
   oracle-pinned score of sx_score_pairs), and searches give the same hits
   with the pre-screen on and off.
+* Packed Viterbi pre-screen (int16x2, two targets of one profile per lane;
+  csrc/prescreen.cuh vit16_kernel): its bound equals the CPU model bit for
+  bit, is never below the reference's f32 Viterbi score (src/hmmer/dp.rs:152-189),
+  and searches give the same hits with the pre-screens on and off.
 * F3 pre-screen (forward_kernel SCAN order): its Forward score differs from
   the exact (reference-order) Forward score by at most the rounding bound the
   cascade adds to its threshold, (L+1)(2M + 6 VC + 64) 2^-24 nats taken
@@ -17,6 +21,7 @@ import sxhmm
 from oracle import oracle as O
 from sxhmm import synth
 from _prescreen_model import msv_bound as model_bound
+from _prescreen_model import vit_bound as vit_model, vit16_width
 from _workloads import edge_targets, fixture_targets, fixture_text, small_config, small_profiles_text, tiny_text
 
 pytestmark = pytest.mark.gpu
@@ -67,6 +72,56 @@ def test_msv_prescreen_bound_model_and_guarantee():
         e.close()
 
 
+def test_vit_prescreen_bound_model_and_guarantee():
+    """Profiles at every pre-screen width's edges (M 20..513), the config-1
+    profiles and the fixture, against background, edge and fixture targets
+    and planted homologs strong enough to reach the int16 cap."""
+    rng = np.random.default_rng(17)
+    w = small_config(1, 0.01)
+    extra = [synth.sample_profile(rng, m, f"v{m}") for m in (20, 32, 33, 64, 65, 128, 200, 256, 300, 511, 512, 513)]
+    text = w.hmm_text() + "".join(synth.profile_text(p) for p in extra) + fixture_text() + tiny_text()
+    seqs = [synth.residues_to_str(s) for s in w.targets[:50]] + [s for _, s in edge_targets()] + \
+        [s for _, s in fixture_targets()]
+    for p in (extra[1], extra[6], extra[10]):
+        dom = synth.emit_homolog(rng, p)
+        seqs.append(synth.residues_to_str(synth.plant(rng, len(dom) + 60, [dom])))
+    o = O.Oracle(text=text)
+    e = sxhmm.Engine()
+    try:
+        ps = e.load_text(text)
+        ts = e.targets(seqs)
+        pp, pt = np.meshgrid(np.arange(o.n), np.arange(len(seqs)), indexing="ij")
+        pp, pt = pp.ravel().astype(np.int32), pt.ravel().astype(np.int32)
+        got = e.score_prescreens(ps, ts, pp, pt)["vit_bound"]
+        exact = e.score_pairs(ps, ts, pp, pt, stages=("viterbi",))["viterbi"]
+        dsq = [O.encode(s) for s in seqs]
+        arrays = [o.arrays(i) for i in range(o.n)]
+        handled = ~np.isnan(got)
+        wide = np.array([vit16_width(o.m[i]) is None for i in pp])
+        empty = np.array([len(dsq[j]) == 0 for j in pt])
+        assert not handled[wide | empty].any()
+        assert handled.sum() > 0.8 * len(pp)
+        # the guarantee on every pair the pre-screen handles
+        assert np.all(got[handled] >= exact[handled]), np.nonzero(got[handled] < exact[handled])
+        assert np.isinf(got[handled]).any(), "no pair reached the cap"
+        # bit-exact with the model on a sample: every profile x every edge,
+        # fixture and homolog target, plus random pairs
+        rng2 = np.random.default_rng(5)
+        pick = np.unique(np.concatenate([rng2.choice(len(pp), 300, replace=False), np.nonzero(pt >= 50)[0]]))
+        for q in pick:
+            i, j = int(pp[q]), int(pt[q])
+            a = arrays[i]
+            want = vit_model(a["msc"], a["t"], o.m[i], dsq[j])
+            assert (np.isnan(want) and np.isnan(got[q])) or want == got[q], (i, j, o.m[i], len(dsq[j]), want, got[q])
+        # the margin on background pairs stays small
+        fin = handled & np.isfinite(got) & np.isfinite(exact)
+        slack = got[fin].astype(np.float64) - exact[fin]
+        print(f"vit bound slack: median {np.median(slack):.3f} nats, 99% {np.quantile(slack, 0.99):.3f}")
+        assert np.median(slack) < 1.0, np.median(slack)
+    finally:
+        e.close()
+
+
 @pytest.mark.parametrize("cfg,scale", [(0, 1.0), (1, 0.01), (4, 0.002)])
 def test_search_prescreen_on_off_identical(cfg, scale):
     w = small_config(cfg, scale)
@@ -88,8 +143,14 @@ def test_search_prescreen_on_off_identical(cfg, scale):
                 assert 0 < st["prescreen"]["pairs_out"] < st["prescreen"]["pairs_in"]
                 # the exact kernel saw exactly the pre-screen's survivors and kept what F1 keeps
                 assert st["pairs_out"][0] <= st["prescreen"]["pairs_out"]
+                # the Viterbi pre-screen bounded bias survivors and passed a subset
+                vp = st["vprescreen"]
+                assert 0 < vp["pairs_in"] <= st["pairs_out"][1]
+                assert vp["pairs_out"] <= vp["pairs_in"]
+                assert st["pairs_out"][2] <= vp["pairs_out"] + (st["pairs_out"][1] - vp["pairs_in"])
             else:
                 assert st["prescreen"]["pairs_in"] == 0
+                assert st["vprescreen"]["pairs_in"] == 0
             out.append(([(h.profile_index, h.target_index, h.score, h.bias, h.evalue, h.ndomains) for h in hits],
                         [(d.score, d.env_from, d.env_to, d.hmm_from, d.hmm_to) for d in doms], st["pairs_out"][0]))
         finally:

@@ -1661,19 +1661,26 @@ void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets*
 }
 
 // Packed Viterbi pre-screen of a block's bias-filter survivors (profiles
-// `prof`, per-profile lists in `vs`): per profile `nsub` strided sub-tiles of
-// its list, larger M first, one launch per shape on the slot's high-priority
-// auxiliary streams; pairs whose bound passes F2 go to the Viterbi lists
-// (lists[2] of stage 1), S.vstats collects cells and passes.
+// `prof`, per-profile lists in `vs`, `count[p - p0]` pairs in each): a
+// profile's list is cut into strided sub-tiles of about twelve rounds of the
+// pairs a CTA holds at once (fewer leave a CTA's slot idle behind its longest
+// target too often), larger M first, one launch per shape on the
+// slot's high-priority auxiliary streams; pairs whose bound passes F2 go to
+// the Viterbi lists (lists[1]), S.vstats collects cells and passes.
 void launch_vprescreen(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T, const std::vector<int>& prof,
-                       const VitScreen& vs) {
+                       const VitScreen& vs, const std::vector<unsigned>& count) {
   const auto& K = kernels();
   std::vector<std::vector<sxk::VitTile>> by_shape(kNumVit16Shapes);
-  const int nsub = std::max(2, std::min(32, (int)std::ceil(8.0 * E->num_sms / std::max<size_t>(1, prof.size()))));
   std::vector<int> order(prof);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return P->h[a].m > P->h[b].m; });
-  for (int pi : order)
+  for (int pi : order) {
+    const unsigned n = std::min(count[pi - vs.p0], vs.cap);
+    if (!n) continue;
+    const Vit16Shape& v = kVit16Shapes[P->dp[pi].qv_shape];
+    const unsigned per = 12u * (unsigned)(vit16_threads(v) / 32) * (unsigned)(32 / v.g) * 2u;  // pairs per sub-tile
+    const int nsub = (int)std::min<unsigned>(256u, (n + per - 1) / per);
     for (int q = 0; q < nsub; q++) by_shape[P->dp[pi].qv_shape].push_back({pi, q, nsub, 0});
+  }
   std::vector<sxk::VitTile> all;
   std::vector<size_t> start(kNumVit16Shapes + 1, 0);
   for (int s = 0; s < kNumVit16Shapes; s++) {
@@ -1689,7 +1696,8 @@ void launch_vprescreen(sx_engine* E, Slot& S, const sx_profiles* P, const sx_tar
     if (start[s + 1] == start[s]) continue;
     const int smem = vit16_smem(kVit16Shapes[s]);
     CK(cudaFuncSetAttribute((const void*)K.vit16[s], cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    K.vit16[s]<<<(unsigned)(start[s + 1] - start[s]), 256, smem, S.hi.aux[lane++ % S.hi.naux]>>>(
+    K.vit16[s]<<<(unsigned)(start[s + 1] - start[s]), vit16_threads(kVit16Shapes[s]), smem,
+                 S.hi.aux[lane++ % S.hi.naux]>>>(
         S.vtiles.p + start[s], P->d_prof.p, E->thr.p, P->d_qvimg.p, T->d_res.p, T->d_off.p, T->d_len.p, T->d_xsc.p,
         vs.list, vs.cap, vs.count, vs.p0, S.lists[1].p, S.bins[1].p, S.counts.p + kMaxBins, S.overflow.p, kSlackBits,
         nullptr, S.vstats.p);
@@ -2115,7 +2123,7 @@ void long_rows(sx_engine* E, const sx_profiles* P, const sx_targets* T, const st
 std::vector<std::pair<int, int>> profile_blocks(const sx_engine* E, const sx_profiles* P, const sx_targets* T,
                                                 const std::vector<Thresholds>& th) {
   constexpr double kCellsPerBlock = 2.5e11;  // ~80 ms of B200 cascade
-  constexpr int kMaxBlocks = 8;
+  constexpr int kMaxBlocks = 5;  // more blocks cost more than their shorter tail saves
   const int np = (int)P->h.size();
   std::vector<double> w(np, 0.0);
   double total = 0;
@@ -2131,11 +2139,22 @@ std::vector<std::pair<int, int>> profile_blocks(const sx_engine* E, const sx_pro
   int nb = E->pipeline_blocks > 0 ? E->pipeline_blocks
                                   : (int)std::min<double>(kMaxBlocks, std::max(1.0, std::floor(total / kCellsPerBlock)));
   nb = std::max(1, std::min(nb, nfilt));
+  // relative block sizes: the last two blocks of an automatic partition of
+  // four or more are smaller (0.6 and 0.3 of the others), so the work left
+  // after the last MSV stage -- that block's later device stages and its
+  // domain definition on the host -- is short
+  std::vector<double> rel(nb, 1.0);
+  if (E->pipeline_blocks <= 0 && nb >= 4) {
+    rel[nb - 2] = 0.6;
+    rel[nb - 1] = 0.3;
+  }
+  std::vector<double> cum(nb + 1, 0.0);
+  for (int b = 0; b < nb; b++) cum[b + 1] = cum[b] + rel[b];
   int p0 = 0;
   double acc = 0;
   for (int pi = 0; pi < np; pi++) {
     acc += w[pi];
-    if ((int)out.size() < nb - 1 && acc >= total * (double)(out.size() + 1) / nb) {
+    if ((int)out.size() < nb - 1 && acc >= total * cum[out.size() + 1] / cum[nb]) {
       out.emplace_back(p0, pi + 1);
       p0 = pi + 1;
     }
@@ -2273,7 +2292,10 @@ bool cascade_finish(sx_engine* E, Slot& S, const sx_profiles* P, const sx_target
       const VitScreen vs{S.vlist.p, R.rcap, S.vcount.p, R.p0};
       launch_stage(E, S, P, T, si, nin, vs);
       CK(cudaEventRecord(S.bias_done, s));
-      launch_vprescreen(E, S, P, T, R.vscreened, vs);
+      std::vector<unsigned> vc((size_t)(R.p1 - R.p0));
+      CK(cudaMemcpyAsync(vc.data(), S.vcount.p, sizeof(unsigned) * vc.size(), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      launch_vprescreen(E, S, P, T, R.vscreened, vs, vc);
       CK(cudaEventRecord(S.vpre_done, s));
       continue;
     }
@@ -3413,7 +3435,7 @@ int sx_score_prescreens(sx_engine* e, const sx_profiles* p, const sx_targets* t,
           const int sh = p->dp[profs[q]].qv_shape;
           const int smem = vit16_smem(kVit16Shapes[sh]);
           CK(cudaFuncSetAttribute((const void*)K.vit16[sh], cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-          K.vit16[sh]<<<kSub, 256, smem, s>>>(S.vtiles.p + q * kSub, p->d_prof.p, e->thr.p, p->d_qvimg.p, t->d_res.p,
+          K.vit16[sh]<<<kSub, vit16_threads(kVit16Shapes[sh]), smem, s>>>(S.vtiles.p + q * kSub, p->d_prof.p, e->thr.p, p->d_qvimg.p, t->d_res.p,
                                              t->d_off.p, t->d_len.p, t->d_xsc.p, S.vlist.p + seg[q], cnt[q],
                                              S.vcount.p + q, profs[q], nullptr, nullptr, nullptr, e->overflow.p,
                                              kSlackBits, e->scores.p, nullptr);

@@ -329,7 +329,7 @@ __device__ __forceinline__ unsigned set_half(unsigned w, int h, unsigned v) {
 // accumulate the DP cells bounded, the cells of the passing pairs and the
 // passing pairs.
 template <int G, int C>
-__global__ void __launch_bounds__(256, (C <= 8 ? 2 : 1)) vit16_kernel(
+__global__ void __launch_bounds__(128, (C <= 8 ? 4 : 3)) vit16_kernel(
     const VitTile* __restrict__ tiles, const DevProfile* __restrict__ profs, const Thresholds* __restrict__ thr,
     const uint4* __restrict__ qvimg, const uint8_t* __restrict__ res, const int64_t* __restrict__ toff,
     const int32_t* __restrict__ tlen, const float4* __restrict__ xsc, const PairRec* __restrict__ vlist,
@@ -378,7 +378,12 @@ __global__ void __launch_bounds__(256, (C <= 8 ? 2 : 1)) vit16_kernel(
   int xn[2] = {0, 0}, xj[2] = {kQ32Neg, kQ32Neg}, fin[2] = {kQ32Neg, kQ32Neg}, tl[2] = {0, 0}, tm[2] = {0, 0};
   bool act[2] = {false, false}, big[2] = {false, false}, dn[2] = {false, false};
   const uint8_t* seq[2] = {res, res};
+  // residues: 16-byte words, the next one prefetched; wc = the current 4
+  // bytes, consumed from the low byte up (targets are padded with '*' to a
+  // 16-byte boundary and followed by 64 bytes of slack, so every byte read is
+  // a valid residue code)
   uint4 rc[2], rn[2];
+  uint32_t wc[2] = {0x18181818u, 0x18181818u};
 #pragma unroll
   for (int h = 0; h < 2; h++) rc[h] = rn[h] = make_uint4(0x18181818u, 0x18181818u, 0x18181818u, 0x18181818u);
   double cells_in = 0.0, cells_pass = 0.0, npass = 0.0;
@@ -424,6 +429,7 @@ __global__ void __launch_bounds__(256, (C <= 8 ? 2 : 1)) vit16_kernel(
           boff[h] = 0;
           rc[h] = __ldg(reinterpret_cast<const uint4*>(seq[h]));
           rn[h] = __ldg(reinterpret_cast<const uint4*>(seq[h] + 16));
+          wc[h] = rc[h].x;
           act[h] = true;
 #pragma unroll
           for (int c = 0; c < C; c++) {
@@ -445,14 +451,10 @@ __global__ void __launch_bounds__(256, (C <= 8 ? 2 : 1)) vit16_kernel(
     }
     if (__all_sync(kFull, dn[0] && dn[1])) break;
 
-    // this row's residue of each half ('*' past the end and for idle halves)
+    // this row's residue of each half (idle halves compute on stale ones)
     int x[2];
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int q = row[h] - boff[h];
-      const uint32_t w = (q >> 2) == 0 ? rc[h].x : (q >> 2) == 1 ? rc[h].y : (q >> 2) == 2 ? rc[h].z : rc[h].w;
-      x[h] = (act[h] && row[h] < L[h]) ? (int)((w >> (8 * (q & 3))) & 0xffu) : 24;
-    }
+    for (int h = 0; h < 2; h++) x[h] = (int)(wc[h] & 0xffu);
     // match scores of both halves, interleaved into words
     unsigned ew[C];
     {
@@ -569,10 +571,16 @@ __global__ void __launch_bounds__(256, (C <= 8 ? 2 : 1)) vit16_kernel(
       b16[h] = max((xb + 2047) >> (kQ32Shift - kQ16Shift), kV16BFloor);
       row[h]++;
       if (row[h] == L[h]) fin[h] = xj[h] + tm[h];
-      if (row[h] - boff[h] == 16) {
-        boff[h] += 16;
-        rc[h] = rn[h];
-        if (act[h]) rn[h] = __ldg(reinterpret_cast<const uint4*>(seq[h] + boff[h] + 16));
+      if ((row[h] & 3) == 0) {
+        if (row[h] - boff[h] == 16) {
+          boff[h] += 16;
+          rc[h] = rn[h];
+          if (act[h]) rn[h] = __ldg(reinterpret_cast<const uint4*>(seq[h] + boff[h] + 16));
+        }
+        const int q = (row[h] - boff[h]) >> 2;
+        wc[h] = q == 0 ? rc[h].x : q == 1 ? rc[h].y : q == 2 ? rc[h].z : rc[h].w;
+      } else {
+        wc[h] >>= 8;
       }
     }
     bw = __byte_perm((unsigned)b16[0], (unsigned)b16[1], 0x5410);

@@ -65,6 +65,9 @@ constexpr int kNumVit16Shapes = sizeof(kVit16Shapes) / sizeof(kVit16Shapes[0]);
 // dynamic shared memory of one tile: 8 transition rows of 4 bytes per column
 // and 25 score rows of 2 bytes per column
 constexpr int vit16_smem(const Vit16Shape& v) { return 82 * v.g * v.c; }
+// threads per CTA: the kernel's launch bounds give 128 registers a thread
+// for C <= 8 (four 128-thread CTAs per SM), 168 for C = 16 (three)
+constexpr int vit16_threads(const Vit16Shape&) { return 128; }
 
 // Warp-chunked column counts (columns per lane, 32 lanes per pair).
 constexpr int kVcBins[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64};

@@ -19,8 +19,9 @@ OBJ = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 # the kernel instantiations sit in their own translation units so they
 # compile in parallel
-SOURCES = ["engine.cu", "k_msv.cu", "k_msv16.cu", "k_vit16.cu", "k_vit.cu", "k_vbin.cu", "k_env.cu", "hmmfile.cpp", "domains.cpp"]
-HEADERS = ["kernels.cuh", "adjoint.cuh", "plain.cuh", "long.cuh", "envelope.cuh", "internal.hpp", "shapes.hpp", "prescreen.cuh",
+SOURCES = ["engine.cu", "pack.cu", "scheduler.cu", "domain_passes.cu", "score.cu", "static_entry.cu", "k_msv.cu",
+           "k_msv16.cu", "k_vit16.cu", "k_vit.cu", "k_vbin.cu", "k_env.cu", "hmmfile.cpp", "domains.cpp"]
+HEADERS = ["engine.hpp", "kernels.cuh", "adjoint.cuh", "plain.cuh", "long.cuh", "envelope.cuh", "internal.hpp", "shapes.hpp", "prescreen.cuh",
            "tuned_shapes.inc"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

@@ -25,7 +25,7 @@ struct LongPair {
 };
 
 // MSV (src/hmmer/dp.rs:92-145): score of every pair.
-__global__ void __launch_bounds__(kPlainThreads) long_msv_kernel(
+static __global__ void __launch_bounds__(kPlainThreads) long_msv_kernel(
     const LongPair* __restrict__ pairs, int n, const PlainProfile* __restrict__ pprof, const float* __restrict__ pimg,
     const DevProfile* __restrict__ profs, const uint8_t* __restrict__ res, const int64_t* __restrict__ toff,
     const int32_t* __restrict__ tlen, const float4* __restrict__ tpar, float* __restrict__ scratch, int64_t stride,
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(kPlainThreads) long_msv_kernel(
 }
 
 // Viterbi filter (src/hmmer/dp.rs:152-189): score of every pair.
-__global__ void __launch_bounds__(kPlainThreads) long_viterbi_kernel(
+static __global__ void __launch_bounds__(kPlainThreads) long_viterbi_kernel(
     const LongPair* __restrict__ pairs, int n, const PlainProfile* __restrict__ pprof, const float* __restrict__ pimg,
     const uint8_t* __restrict__ res, const int64_t* __restrict__ toff, const int32_t* __restrict__ tlen,
     const float4* __restrict__ xsc, float* __restrict__ scratch, int64_t stride, float* __restrict__ out) {
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(kPlainThreads) long_viterbi_kernel(
 // pair, multihit, writing the raw special rows exactly as forward_kernel and
 // backward_kernel do: fwd rows 1..L (N B E J C, rescale factor or 0); bwd
 // row L (E, C), rows L-1..1 (N B E J C, factor) and the B sum in slot 1 of row 0.
-__global__ void __launch_bounds__(kPlainThreads) long_rows_kernel(
+static __global__ void __launch_bounds__(kPlainThreads) long_rows_kernel(
     const LongPair* __restrict__ pairs, int n, const PlainProfile* __restrict__ pprof, const float* __restrict__ pimg,
     const uint8_t* __restrict__ res, const int64_t* __restrict__ toff, const int32_t* __restrict__ tlen,
     const float4* __restrict__ xsc, float* __restrict__ scratch, int64_t stride, float* __restrict__ rows_f,

@@ -35,7 +35,7 @@ __device__ __forceinline__ float block_max(float v, float* red) {
 }
 
 // MSV (src/hmmer/dp.rs:92-145) for pairs p = first_p + blockIdx.x / nt, t = blockIdx.x % nt.
-__global__ void __launch_bounds__(kPlainThreads) plain_msv_kernel(
+static __global__ void __launch_bounds__(kPlainThreads) plain_msv_kernel(
     int64_t first_pair, int nt, const PlainProfile* __restrict__ pprof, const float* __restrict__ pimg,
     const DevProfile* __restrict__ profs, const Thresholds* __restrict__ thr, const uint8_t* __restrict__ res,
     const int64_t* __restrict__ toff, const int32_t* __restrict__ tlen, const float4* __restrict__ tpar,
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kPlainThreads) plain_msv_kernel(
 
 // Viterbi (src/hmmer/dp.rs:152-189), one CTA per pair of the input list; the
 // row's D chain is run serially by thread 0.
-__global__ void __launch_bounds__(kPlainThreads) plain_viterbi_kernel(
+static __global__ void __launch_bounds__(kPlainThreads) plain_viterbi_kernel(
     const PairRec* __restrict__ in, const unsigned* __restrict__ in_counts, const BinRegion* __restrict__ in_bins,
     int bin, PairRec* __restrict__ out, const BinRegion* __restrict__ out_bins, unsigned* __restrict__ out_counts,
     unsigned* __restrict__ overflow, const PlainProfile* __restrict__ pprof, const float* __restrict__ pimg,

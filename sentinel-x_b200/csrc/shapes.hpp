@@ -2,7 +2,7 @@
 //
 // The template instantiations live in their own translation units
 // (k_msv.cu, k_msv16.cu, k_vit.cu, k_vit16.cu, k_vbin.cu, k_env.cu) so the library builds in
-// parallel; engine.cu launches them through the function-pointer tables
+// parallel; the host translation units launch them through the function-pointer tables
 // filled here.
 #pragma once
 #include <cstdint>

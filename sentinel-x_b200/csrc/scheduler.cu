@@ -513,9 +513,9 @@ void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets*
 
 // Packed Viterbi pre-screen of a block's bias-filter survivors (profiles
 // `prof`, per-profile lists in `vs`, `count[p - p0]` pairs in each): a
-// profile's list is cut into strided sub-tiles of about twelve rounds of the
-// pairs a CTA holds at once (fewer leave a CTA's slot idle behind its longest
-// target too often), larger M first, one launch per shape on the
+// profile's list is cut into strided sub-tiles of about 24 rounds of the
+// pairs a CTA holds at once (with 6 a CTA's slot idles behind its longest
+// target too often: 69 ms against 59), larger M first, one launch per shape on the
 // slot's high-priority auxiliary streams; pairs whose bound passes F2 go to
 // the Viterbi lists (lists[1]), S.vstats collects cells and passes.
 void launch_vprescreen(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets* T, const std::vector<int>& prof,
@@ -528,7 +528,7 @@ void launch_vprescreen(sx_engine* E, Slot& S, const sx_profiles* P, const sx_tar
     const unsigned n = std::min(count[pi - vs.p0], vs.cap);
     if (!n) continue;
     const Vit16Shape& v = kVit16Shapes[P->dp[pi].qv_shape];
-    const unsigned per = 12u * (unsigned)(vit16_threads(v) / 32) * (unsigned)(32 / v.g) * 2u;  // pairs per sub-tile
+    const unsigned per = 24u * (unsigned)(vit16_threads(v) / 32) * (unsigned)(32 / v.g) * 2u;  // pairs per sub-tile
     const int nsub = (int)std::min<unsigned>(256u, (n + per - 1) / per);
     for (int q = 0; q < nsub; q++) by_shape[P->dp[pi].qv_shape].push_back({pi, q, nsub, 0});
   }

@@ -56,11 +56,14 @@ static_assert(kNumVitShapes <= kMaxBins, "too many Viterbi shapes");
 
 // Packed Viterbi pre-screen shapes (prescreen.cuh vit16_kernel): G lanes per
 // pair of targets, C columns per lane; a profile takes the narrowest that
-// covers M, profiles wider than the last one are not pre-screened.
+// covers M, profiles wider than the last one are not pre-screened.  Above 64
+// columns 16 columns a lane beat 8 (Viterbi pre-screen of the Pfam-scale
+// search 65 -> 59 ms): the row's per-lane overhead is shared by twice the
+// cells, at 163 registers and three 128-thread CTAs per SM.
 struct Vit16Shape {
   int g, c;
 };
-constexpr Vit16Shape kVit16Shapes[] = {{4, 8}, {8, 8}, {16, 8}, {32, 8}, {32, 16}};
+constexpr Vit16Shape kVit16Shapes[] = {{4, 8}, {8, 8}, {8, 16}, {16, 16}, {32, 16}};
 constexpr int kNumVit16Shapes = sizeof(kVit16Shapes) / sizeof(kVit16Shapes[0]);
 // dynamic shared memory of one tile: 8 transition rows of 4 bytes per column
 // and 25 score rows of 2 bytes per column

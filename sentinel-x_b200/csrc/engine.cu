@@ -311,18 +311,46 @@ int sx_targets_create_digital(sx_engine* e, const uint8_t* dsq, const int64_t* o
     total += ((size_t)lens[i] + 15) & ~(size_t)15;
   }
   t->dsq = e->target_bytes.take(total);
-  t->off.reserve(n);
-  t->len.reserve(n);
+  // packed offsets first; then each target is checked, copied and padded
+  // with '*' to its 16-byte boundary, targets spread over the host threads
+  // (sets of a few MB and more: a Pfam-scale set of 50,000 targets is
+  // repacked for every search of a streaming caller)
+  t->off.resize(n);
+  t->len.resize(n);
+  int64_t o = 0;
   for (size_t i = 0; i < n; i++) {
+    t->off[i] = o;
+    t->len[i] = (int32_t)lens[i];
+    o += (lens[i] + 15) & ~(int64_t)15;
+  }
+  t->dsq.resize((size_t)o);
+  uint8_t* out8 = t->dsq.data();
+  std::atomic<size_t> bad{SIZE_MAX};
+  const size_t nchunk = o >= (1 << 22) ? std::min<size_t>(n, 8 * (size_t)e->host_threads) : 1;
+  parallel_for(nchunk, e->host_threads, [&](size_t c) {
+    for (size_t i = n * c / nchunk; i < n * (c + 1) / nchunk; i++) {
+      const uint8_t* d = dsq + offsets[i];
+      uint8_t hi = 0;  // max code, a loop the compiler vectorises; positions only on failure
+      for (int64_t q = 0; q < lens[i]; q++) hi = std::max(hi, d[q]);
+      if (hi > SYM_STAR) {
+        size_t cur = bad.load();
+        while (i < cur && !bad.compare_exchange_weak(cur, i)) {
+        }
+        return;
+      }
+      uint8_t* w = out8 + t->off[i];
+      if (lens[i]) std::memcpy(w, d, (size_t)lens[i]);
+      const int64_t pad = ((lens[i] + 15) & ~(int64_t)15) - lens[i];
+      if (pad) std::memset(w + lens[i], SYM_STAR, (size_t)pad);
+    }
+  });
+  if (bad.load() != SIZE_MAX) {
+    const size_t i = bad.load();
     const uint8_t* d = dsq + offsets[i];
-    uint8_t hi = 0;  // max code, a loop the compiler vectorises; positions only on failure
-    for (int64_t q = 0; q < lens[i]; q++) hi = std::max(hi, d[q]);
-    if (hi > SYM_STAR)
-      for (int64_t q = 0; q < lens[i]; q++)
-        if (d[q] > SYM_STAR)
-          return fail(SX_EINVAL, "sx_targets_create_digital: residue code " + std::to_string(d[q]) +
-                                     " out of range in target " + std::to_string(i));
-    append_target(t.get(), d, (size_t)lens[i]);
+    for (int64_t q = 0; q < lens[i]; q++)
+      if (d[q] > SYM_STAR)
+        return fail(SX_EINVAL, "sx_targets_create_digital: residue code " + std::to_string(d[q]) +
+                                   " out of range in target " + std::to_string(i));
   }
   return finish_targets(e, std::move(t), out);
 }

@@ -210,22 +210,63 @@ float f32_boundary(Pred pass) {
 // pair (and the device-wide synchronisation of cudaFree) per batch.
 // Host buffers of packed residues, recycled across target sets so that a
 // caller streaming batches of targets writes into pages already touched.
+// Page-locked host memory for the packed residues of target sets, so their
+// copy to the device runs at the bus's rate rather than through the driver's
+// pageable staging; plain heap memory when the pinned allocation fails.
+// Growing a vector leaves the new elements uninitialised (the packers write
+// every byte).
+template <typename T>
+struct PinnedAlloc {
+  using value_type = T;
+  PinnedAlloc() = default;
+  template <typename U>
+  PinnedAlloc(const PinnedAlloc<U>&) {}
+  T* allocate(size_t n) {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, std::max<size_t>(n, 1) * sizeof(T), cudaHostAllocDefault) == cudaSuccess) return static_cast<T*>(p);
+    cudaGetLastError();
+    p = std::malloc(std::max<size_t>(n, 1) * sizeof(T));
+    if (!p) throw std::bad_alloc();
+    return static_cast<T*>(p);
+  }
+  void deallocate(T* p, size_t) {
+    unsigned flags = 0;
+    if (cudaHostGetFlags(&flags, p) == cudaSuccess) {
+      cudaFreeHost(p);
+    } else {
+      cudaGetLastError();
+      std::free(p);
+    }
+  }
+  template <typename U>
+  void construct(U* p) noexcept {}  // default-initialise: no fill
+  template <typename U, typename... A>
+  void construct(U* p, A&&... a) {
+    ::new ((void*)p) U(std::forward<A>(a)...);
+  }
+  template <typename U>
+  bool operator==(const PinnedAlloc<U>&) const { return true; }
+  template <typename U>
+  bool operator!=(const PinnedAlloc<U>&) const { return false; }
+};
+using HostBytes = std::vector<uint8_t, PinnedAlloc<uint8_t>>;
+
 class HostBytePool {
  public:
-  std::vector<uint8_t> take(size_t bytes) {
+  HostBytes take(size_t bytes) {
     std::lock_guard<std::mutex> g(mu_);
     for (size_t i = 0; i < free_.size(); i++)
       if (free_[i].capacity() >= bytes) {
-        std::vector<uint8_t> v = std::move(free_[i]);
+        HostBytes v = std::move(free_[i]);
         free_.erase(free_.begin() + (std::ptrdiff_t)i);
         v.clear();
         return v;
       }
-    std::vector<uint8_t> v;
+    HostBytes v;
     v.reserve(bytes);
     return v;
   }
-  void give(std::vector<uint8_t>&& v) {
+  void give(HostBytes&& v) {
     if (!v.capacity()) return;
     std::lock_guard<std::mutex> g(mu_);
     free_.push_back(std::move(v));
@@ -236,7 +277,7 @@ class HostBytePool {
 
  private:
   std::mutex mu_;
-  std::vector<std::vector<uint8_t>> free_;
+  std::vector<HostBytes> free_;
 };
 
 class BlockPool {
@@ -489,7 +530,7 @@ struct sx_profiles {
 struct sx_targets {
   sx_engine* eng = nullptr;
   std::vector<std::string> ids;  // caller's names (sx_targets_create); empty for digital sets
-  std::vector<uint8_t> dsq;  // packed digital residues, each target 16-byte aligned
+  HostBytes dsq;  // packed digital residues, each target 16-byte aligned (page-locked)
   std::vector<int64_t> off;
   std::vector<int32_t> len;
   std::vector<int32_t> order;  // indices sorted by length, longest first

@@ -525,6 +525,12 @@ struct sx_profiles {
   DevBuf<uint4> d_qvimg;  // quantized Viterbi images of the packed pre-screen
   DevBuf<float> d_vfb;
   DevBuf<double> d_bias;
+  // the filter thresholds of the last search options seen (they depend on the
+  // profiles' statistics and F1/F2/F3 alone): a stream of searches with one
+  // configuration computes them once
+  mutable std::mutex th_mu;
+  mutable std::vector<Thresholds> th_cache;
+  mutable double th_key[4] = {-1, -1, -1, -1};
 };
 
 struct sx_targets {

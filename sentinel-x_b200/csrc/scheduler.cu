@@ -946,7 +946,16 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
   o.f3 = cfg->f3;
   const size_t np = P->h.size(), nt = T->len.size();
   cudaStream_t s = E->stream;
-  std::vector<Thresholds> th = make_thresholds(P->h, o);
+  std::vector<Thresholds> th;
+  {
+    const double key[4] = {o.filters ? 1.0 : 0.0, o.f1, o.f2, o.f3};
+    std::lock_guard<std::mutex> g(P->th_mu);
+    if (P->th_cache.size() != np || std::memcmp(key, P->th_key, sizeof key) != 0) {
+      P->th_cache = make_thresholds(P->h, o);
+      std::memcpy(P->th_key, key, sizeof key);
+    }
+    th = P->th_cache;
+  }
   // profiles longer than kMaxM take the long pass instead of the cascade
   std::vector<int> longs;
   std::vector<char> long_exact(np, 0);

@@ -61,12 +61,17 @@ struct NvtxRange {
 // clock reads only).
 struct PhaseLog {
   bool on = std::getenv("SXHMM_PROFILE") != nullptr;
+  std::mutex mu;  // entries may come from the host pool's thread
   std::vector<std::pair<std::string, double>> v;
-  void add(const char* name, std::chrono::steady_clock::time_point t0) {
-    if (on) v.emplace_back(name, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
-  }
-  void print() const {
+  void add(const std::string& name, std::chrono::steady_clock::time_point t0) {
     if (!on) return;
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    std::lock_guard<std::mutex> g(mu);
+    v.emplace_back(name, ms);
+  }
+  void print() {
+    if (!on) return;
+    std::lock_guard<std::mutex> g(mu);
     std::string o = "[sxhmm profile]";
     char buf[96];
     for (const auto& p : v) {

@@ -980,6 +980,8 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     std::vector<PairResult> res;
   };
   std::vector<std::unique_ptr<BlockOut>> outs;
+  // with SXHMM_PROFILE: each block's milestones, milliseconds since the call began
+  PhaseLog timeline;
   std::atomic<int64_t> n_domain{0};
   double rows_ms = 0;
   // errors raised on the host pool's thread, reported after it is joined
@@ -1040,10 +1042,18 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     B->res.resize(B->finals.size());
     // the host job of one chunk of rows: `get` hands it the rows (at once, or
     // after waiting for the asynchronous row passes)
-    auto queue_chunk = [&, B, dev_env](std::function<RowsChunk()> get) {
-      hq.push([&, B, dev_env, get](int nthr) {
+    const size_t bi = outs.size() - 1;
+    auto queue_chunk = [&, B, dev_env, bi](std::function<RowsChunk()> get) {
+      hq.push([&, B, dev_env, get, bi](int nthr) {
         try {
           auto ch = std::make_shared<RowsChunk>(get());
+          timeline.add("b" + std::to_string(bi) + "_rows", t_start);
+          struct Done {
+            PhaseLog& tl;
+            size_t bi;
+            std::chrono::steady_clock::time_point t0;
+            ~Done() { tl.add("b" + std::to_string(bi) + "_host", t0); }
+          } done{timeline, bi, t_start};
           const size_t nq = ch->which.size();
           // largest pairs first, for an even finish across the workers
           std::vector<size_t> ord(nq);
@@ -1156,6 +1166,7 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
     outs.push_back(std::make_unique<BlockOut>());
     BlockOut* B = outs.back().get();
     while (!cascade_finish(E, S, P, T, th, o, runs[b], B->finals)) cascade_launch(E, S, P, T, th, runs[b]);
+    timeline.add("b" + std::to_string(b) + "_cascade", t_start);
     nfinal += (int64_t)B->finals.size();
     rows_and_queue(S, B, device_envelopes(B, runs[b].cells_total));
   }
@@ -1286,6 +1297,7 @@ int run_search(sx_engine* E, const sx_profiles* P, const sx_targets* T, const sx
   E->stats.ms[7] = std::chrono::duration<double, std::milli>(t_end - t_dev).count();
   plog.add("total", t_start);
   plog.print();
+  timeline.print();
   std::vector<std::vector<std::pair<int32_t, HitOut>>> per(np);
   for (auto& B : outs) {
     for (const auto& f : B->finals) E->stats.cells[4] += (double)P->h[f.p].m * T->len[f.t];

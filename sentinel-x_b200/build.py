@@ -41,14 +41,16 @@ def compile_cmd(src):
 
 
 def link_cmd():
-    return common() + ["-shared", "-o", OUT] + [obj_of(s) for s in SOURCES] + ["-lz", "-lpthread"]
+    # only the C ABI is exported (csrc/exports.map)
+    return common() + ["-shared", "-o", OUT] + [obj_of(s) for s in SOURCES] + [
+        "-Xlinker", "--version-script=" + os.path.join(CSRC, "exports.map"), "-lz", "-lpthread"]
 
 
 def stale():
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(INCLUDE, "sxhmm.h"), __file__]
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS + ["exports.map"]] + [os.path.join(INCLUDE, "sxhmm.h"), __file__]
     return any(os.path.getmtime(d) > t for d in deps)
 
 

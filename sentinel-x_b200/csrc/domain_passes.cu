@@ -5,6 +5,35 @@
 
 namespace sxe {
 
+// The per-bin launches of a pass fan out over the two slots' high-priority
+// auxiliary streams, idle once the cascade is done: a launch holds only as
+// many warps as its bin has envelopes (tens), and on one stream the bins of a
+// pass would run one after another -- the pass taking the sum of its bins'
+// longest chains instead of the largest one.
+struct FanOut {
+  sx_engine* E;
+  cudaStream_t origin;
+  std::vector<cudaStream_t> lanes;
+  size_t next = 0;
+  FanOut(sx_engine* e, cudaStream_t s) : E(e), origin(s) {
+    CK(cudaEventRecord(E->env_ev, s));
+    for (Slot& S : E->sl) {
+      CK(cudaStreamWaitEvent(S.hi.main, E->env_ev, 0));
+      fork_aux(S.hi);
+      for (int a = 0; a < S.hi.naux; a++) lanes.push_back(S.hi.aux[a]);
+    }
+  }
+  cudaStream_t take() { return lanes[next++ % lanes.size()]; }
+  // the origin stream waits for every launch made
+  void join() {
+    for (Slot& S : E->sl) {
+      join_aux(S.hi);
+      CK(cudaEventRecord(E->env_ev, S.hi.main));
+      CK(cudaStreamWaitEvent(origin, E->env_ev, 0));
+    }
+  }
+};
+
 // The device passes of a DomainBatch: for every envelope request the
 // full-matrix Forward and Backward (their raw special rows come back to the
 // host), the host's posterior factors, then the posterior / null2 /
@@ -88,19 +117,19 @@ int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T,
         x = y;
       }
     };
-    // Forward on the envelope stream, Backward beside it on the second one
-    CK(cudaEventRecord(E->env_ev, s));
-    CK(cudaStreamWaitEvent(E->env_stream2, E->env_ev, 0));
-    each_bin([&](int vb, int x0, int cnt, int blocks) {
-      K.envf[vb]<<<blocks, 32, 0, s>>>(E->env_recs.p + x0, cnt, P->d_prof.p, P->d_vfb.p, T->d_res.p, T->d_off.p,
-                                       E->env_planes.p, E->env_rows.p);
-      K.envb[vb]<<<blocks, 32, 0, E->env_stream2>>>(E->env_recs.p + x0, cnt, P->d_prof.p, P->d_vfb.p, T->d_res.p,
-                                                    T->d_off.p, E->env_planes.p, E->env_rows.p);
-      launches += 2;
-    });
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(E->env_ev, E->env_stream2));
-    CK(cudaStreamWaitEvent(s, E->env_ev, 0));
+    // Forward and Backward of every bin at once, each launch on a stream of its own
+    {
+      FanOut fan(E, s);
+      each_bin([&](int vb, int x0, int cnt, int blocks) {
+        K.envf[vb]<<<blocks, 32, 0, fan.take()>>>(E->env_recs.p + x0, cnt, P->d_prof.p, P->d_vfb.p, T->d_res.p,
+                                                  T->d_off.p, E->env_planes.p, E->env_rows.p);
+        K.envb[vb]<<<blocks, 32, 0, fan.take()>>>(E->env_recs.p + x0, cnt, P->d_prof.p, P->d_vfb.p, T->d_res.p,
+                                                  T->d_off.p, E->env_planes.p, E->env_rows.p);
+        launches += 2;
+      });
+      CK(cudaGetLastError());
+      fan.join();
+    }
     std::vector<float> hrows((size_t)rowsz);
     CK(cudaMemcpyAsync(hrows.data(), E->env_rows.p, sizeof(float) * (size_t)rowsz, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -128,14 +157,16 @@ int64_t envelope_passes(sx_engine* E, const sx_profiles* P, const sx_targets* T,
     const auto tb2 = std::chrono::steady_clock::now();
     CK(cudaMemcpyAsync(E->env_aux.p, haux.data(), sizeof(float) * (size_t)aux, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(E->env_fac.p, hfac.data(), sizeof(double) * (size_t)fac, cudaMemcpyHostToDevice, s));
+    FanOut fan(E, s);
     each_bin([&](int vb, int x0, int cnt, int blocks) {
       const size_t psm = sxk::env_post_smem(kVcBins[vb]);
       CK(cudaFuncSetAttribute((const void*)K.envp[vb], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
-      K.envp[vb]<<<blocks, 32, psm, s>>>(E->env_recs.p + x0, cnt, P->d_prof.p, P->d_vfb.p, E->env_planes.p,
+      K.envp[vb]<<<blocks, 32, psm, fan.take()>>>(E->env_recs.p + x0, cnt, P->d_prof.p, P->d_vfb.p, E->env_planes.p,
                                        E->env_aux.p, E->env_fac.p, E->env_out.p);
       launches += 1;
     });
     CK(cudaGetLastError());
+    fan.join();
     std::vector<float> hout(n * sxk::kEnvOut);
     CK(cudaMemcpyAsync(hout.data(), E->env_out.p, sizeof(float) * hout.size(), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -259,17 +290,20 @@ RegionPassStats region_passes(sx_engine* E, const sx_profiles* P, const sx_targe
     E->trc_status.alloc(n);
     CK(cudaMemsetAsync(E->trc_count.p, 0, sizeof(int32_t), s));
     // the region Forward passes, one launch per vbin (regions are sorted by
-    // vbin), then one trace launch over the batch
+    // vbin) on streams of their own, then one trace launch over the batch
+    FanOut fan(E, s);
     for (size_t x = 0; x < n;) {
       const int vb = P->dp[reg(order[a + x]).p].vbin;
       size_t y = x;
       while (y < n && P->dp[reg(order[a + y]).p].vbin == vb) y++;
       const int cnt = (int)(y - x);
-      K.regf[vb]<<<(int)std::min<int64_t>(cnt, (int64_t)E->num_sms * 32), 32, 0, s>>>(
+      K.regf[vb]<<<(int)std::min<int64_t>(cnt, (int64_t)E->num_sms * 32), 32, 0, fan.take()>>>(
           E->env_recs.p + x, cnt, P->d_prof.p, P->d_vfb.p, T->d_res.p, T->d_off.p, E->env_planes.p, E->env_rows.p);
       st.launches += 1;
       x = y;
     }
+    CK(cudaGetLastError());
+    fan.join();
     sxk::env_trace_kernel<<<(int)std::min<int64_t>(((int64_t)n + 3) / 4, (int64_t)E->num_sms * 16), 128, 0, s>>>(
         E->trc_recs.p, (int)n, E->trc_cols.p, T->d_res.p, T->d_off.p, E->env_planes.p, E->env_rows.p, E->env_aux.p,
         E->trc_pool.p, E->trc_count.p, (int32_t)pool_cap, 0, E->trc_status.p, tc);

@@ -81,7 +81,6 @@ int sx_create(const sx_opts* opts, sx_engine** out) {
       int least = 0, greatest = 0;
       CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
       CK(cudaStreamCreateWithPriority(&e->env_stream, cudaStreamNonBlocking, greatest));
-      CK(cudaStreamCreateWithPriority(&e->env_stream2, cudaStreamNonBlocking, greatest));
       CK(cudaEventCreateWithFlags(&e->env_ev, cudaEventDisableTiming));
     }
     note_free_memory(e.get());
@@ -98,13 +97,12 @@ void sx_destroy(sx_engine* e) {
   if (!e) return;
   cudaSetDevice(e->device);
   for (Slot& S : e->sl) S.destroy();
-  for (cudaStream_t st : {e->env_stream, e->env_stream2})
-    if (st) {
-      cudaStreamSynchronize(st);
-      cudaStreamDestroy(st);
-    }
+  if (e->env_stream) {
+    cudaStreamSynchronize(e->env_stream);
+    cudaStreamDestroy(e->env_stream);
+  }
   if (e->env_ev) cudaEventDestroy(e->env_ev);
-  e->env_stream = e->env_stream2 = nullptr;
+  e->env_stream = nullptr;
   e->env_ev = nullptr;
   bool last;
   {

@@ -119,11 +119,23 @@ struct DevBuf {
     n = count;
     owned = false;
   }
-  void alloc(size_t count) {  // grow-only, contents undefined
+  // Grow-only, contents undefined.  A buffer that must grow takes a quarter
+  // more than asked: the scratch of a stream of searches (survivor lists,
+  // envelope planes) varies from call to call, and each regrowth is a
+  // cudaFree -- which waits for the whole device -- and a fresh cudaMalloc.
+  void alloc(size_t count) {
     if (count <= n && p) return;
     release();
-    CK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
-    n = std::max<size_t>(count, 1);
+    const size_t want = std::max<size_t>(count, 1);
+    const size_t ask = want + want / 4;
+    if (cudaMalloc(&p, ask * sizeof(T)) == cudaSuccess) {
+      n = ask;
+      return;
+    }
+    cudaGetLastError();
+    p = nullptr;
+    CK(cudaMalloc(&p, want * sizeof(T)));
+    n = want;
   }
   void upload(const T* src, size_t count, cudaStream_t s) {
     alloc(count);
@@ -418,8 +430,8 @@ struct Slot {
   void create() {
     int least = 0, greatest = 0;
     CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    // 2 slots x (9 + 6) streams + 2 envelope streams = 32, the
-    // most hardware work queues a process can have (CUDA_DEVICE_MAX_CONNECTIONS=32):
+    // 2 slots x (9 + 6) streams + 1 envelope stream = 31, within the 32
+    // hardware work queues a process can have (CUDA_DEVICE_MAX_CONNECTIONS=32):
     // with fewer queues, streams share them and a high-priority launch can
     // wait behind queued MSV work
     hi.create(greatest, 8);
@@ -494,7 +506,7 @@ struct sx_engine {
   HostBytePool target_bytes;  // host residue buffers of freed target sets
   // envelope passes of the host domain definition (used by the host pool's
   // driver thread, one batch at a time)
-  cudaStream_t env_stream = nullptr, env_stream2 = nullptr;  // Backward runs beside Forward
+  cudaStream_t env_stream = nullptr;  // the passes' copies; their launches fan out over the slots' streams
   cudaEvent_t env_ev = nullptr;
   DevBuf<sxk::EnvRec> env_recs;
   DevBuf<float> env_planes, env_rows, env_aux, env_out;

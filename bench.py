@@ -467,10 +467,12 @@ def marker_set_run(sxhmm, local, torch, ngenomes, prescreen=True, envelopes="aut
             "per_genome": {"final_pairs": round(pin[4] / ng, 1), "envelopes_on_device": round(pout[5] / ng, 1),
                            "regions_to_device": round(pin[6] / ng, 1), "regions_traced_on_device": round(pout[6] / ng, 1)},
             "placement": {"envelopes": envelopes, "traces": traces},
-            "host_gap_ms_per_genome": round(wall - critical, 2),
+            "host_gap_ms_per_genome": round(max(0.0, wall - critical), 2),
             "host_gap_note": "median wall (target upload + search + hits) minus the device stages on the critical "
-                             "path (MSV, bias, Viterbi, Forward pre-screen, row passes) and the host tail: an upper "
-                             "bound on launch, copy and synchronisation overhead per search"}
+                             "path (MSV, bias, Viterbi, Forward pre-screen, row passes) and the host tail (which "
+                             "includes the envelopes' device passes): an upper bound on launch, copy and "
+                             "synchronisation overhead per search; 0 when those stages already cover the wall time "
+                             "(they overlap, so their sum can exceed it)"}
 
 
 def main():

@@ -14,6 +14,10 @@ value  = sum over pairs of M*L / device time of the step (inputs resident on
          the device, L2 flushed between steps), whole job over all ranks.
 e2e    = same metric through the public C ABI with host buffers: digitised
          targets copied host->device, search, hits read back, every step.
+         The profile set stays loaded on the device across steps, as a
+         library serving a stream of searches keeps it (loading it once per
+         profile file is the reference's use too: search_hmm_file parses a
+         library once per call, then searches every target batch).
 Under torchrun (N > 1) each rank searches its own block of 1,000 profiles
 against the same targets (profile-block sharding, no data-path collective).
 """
@@ -28,8 +32,8 @@ import sys
 import threading
 import time
 
-# The engine drives up to 32 streams (two pipeline slots, high- and
-# low-priority sets); give the process that many hardware work queues before
+# The engine drives up to 31 streams (two pipeline slots, high- and
+# low-priority sets, and the domain passes' copy stream); give the process 32 hardware work queues before
 # anything initialises CUDA, so high-priority stages never queue behind MSV.
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 

@@ -113,15 +113,33 @@ std::function<RowsChunk()> rows_pass_async(sx_engine* E, Slot& S, const sx_profi
   // rows the kernels never touch are zero
   CK(cudaMemsetAsync(S.rows_f.p, 0, sizeof(float) * (size_t)ro, s));
   CK(cudaMemsetAsync(S.rows_b.p, 0, sizeof(float) * (size_t)ro, s));
-  fork_aux(S.hi);
+  // Each launch lasts about its longest chain (rows x columns of its
+  // longest pair); the launches go longest first to the least-loaded
+  // auxiliary stream, so the long bins start at once and the short ones
+  // queue behind other short ones
+  std::vector<double> load(S.hi.naux, 0.0);
+  auto pick_stream = [&](double est) {
+    const int a = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    load[a] += est;
+    return S.hi.aux[a];
+  };
+  std::vector<std::pair<double, int>> order;
   for (int b = 0; b < kNumVbins; b++) {
     if (!cnt[b]) continue;
+    int64_t longest = 0;
+    for (size_t i : byb[b]) longest = std::max<int64_t>(longest, T->len[pairs[i].t]);
+    order.emplace_back((double)longest * kVcBins[b], b);
+  }
+  std::stable_sort(order.begin(), order.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+  fork_aux(S.hi);
+  for (const auto& ob : order) {
+    const int b = ob.second;
     // The row passes are latency-bound chains that run for milliseconds
     // beside the next block's MSV: packed kRowsWarps to a CTA they hold the
     // registers of a few SMs instead of one MSV CTA slot on nearly every SM.
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)cnt[b] + kRowsWarps - 1) / kRowsWarps,
                                                                    (int64_t)E->num_sms * 32 / kRowsWarps));
-    cudaStream_t sa = S.hi.aux[(2 * b) % S.hi.naux], sb = S.hi.aux[(2 * b + 1) % S.hi.naux];
+    cudaStream_t sa = pick_stream(ob.first), sb = pick_stream(ob.first);
     K.fwd[b]<<<blocks, 32 * kRowsWarps, 0, sa>>>(S.rrecs.p, S.rcnt.p, S.rbins.p, b, nullptr, nullptr, nullptr, S.overflow.p,
                                      P->d_prof.p, E->thr.p, P->d_vfb.p, T->d_res.p, T->d_off.p, T->d_len.p,
                                      T->d_xsc.p, 0.f, S.rows_f.p, S.roff.p);

@@ -498,11 +498,19 @@ void launch_stage(sx_engine* E, Slot& S, const sx_profiles* P, const sx_targets*
       CK(cudaMemsetAsync(S.cursor.p, 0, sizeof(unsigned) * kMaxBins, S.hi.main));
     }
     fork_aux(S.hi);
-    int lane = 0;
+    // widest bins first, each to the least-loaded auxiliary stream: a bin's
+    // launch lasts about its longest row chain, which grows with the width
     const int nb = si == 1 ? kNumVitShapes : kNumVbins;
-    for (int b = 0; b < nb; b++) {
-      if (!nin[b]) continue;
-      cudaStream_t s = S.hi.aux[lane++ % S.hi.naux];
+    std::vector<std::pair<int, int>> order;  // (columns, bin)
+    for (int b = 0; b < nb; b++)
+      if (nin[b]) order.emplace_back(si == 1 ? kVitShapes[b].g * kVitShapes[b].c : 32 * kVcBins[b], b);
+    std::stable_sort(order.begin(), order.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<double> load(S.hi.naux, 0.0);
+    for (const auto& ob : order) {
+      const int b = ob.second;
+      const int a = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      load[a] += (double)ob.first;
+      cudaStream_t s = S.hi.aux[a];
       if (si == 1 && (E->flags & SX_FLAG_PLAIN)) {
         sxk::plain_viterbi_kernel<<<(unsigned)std::min<int64_t>(nin[b], (int64_t)E->num_sms * 64), sxk::kPlainThreads,
                                     0, S.hi.main>>>(S.lists[1].p, cin, S.bins[1].p, b, S.lists[2].p, S.bins[2].p,

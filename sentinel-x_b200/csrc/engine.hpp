@@ -238,20 +238,29 @@ struct PinnedAlloc {
   PinnedAlloc() = default;
   template <typename U>
   PinnedAlloc(const PinnedAlloc<U>&) {}
+  // Each block starts with a 64-byte header recording how it was obtained,
+  // so it is freed the same way even after the CUDA context is gone.
+  static constexpr size_t kHead = 64;
   T* allocate(size_t n) {
+    const size_t bytes = std::max<size_t>(n, 1) * sizeof(T) + kHead;
     void* p = nullptr;
-    if (cudaHostAlloc(&p, std::max<size_t>(n, 1) * sizeof(T), cudaHostAllocDefault) == cudaSuccess) return static_cast<T*>(p);
-    cudaGetLastError();
-    p = std::malloc(std::max<size_t>(n, 1) * sizeof(T));
-    if (!p) throw std::bad_alloc();
-    return static_cast<T*>(p);
-  }
-  void deallocate(T* p, size_t) {
-    unsigned flags = 0;
-    if (cudaHostGetFlags(&flags, p) == cudaSuccess) {
-      cudaFreeHost(p);
-    } else {
+    uint32_t pinned = 1;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
       cudaGetLastError();
+      pinned = 0;
+      p = std::malloc(bytes);
+      if (!p) throw std::bad_alloc();
+    }
+    std::memcpy(p, &pinned, sizeof pinned);
+    return reinterpret_cast<T*>(static_cast<char*>(p) + kHead);
+  }
+  void deallocate(T* q, size_t) {
+    void* p = reinterpret_cast<char*>(q) - kHead;
+    uint32_t pinned = 0;
+    std::memcpy(&pinned, p, sizeof pinned);
+    if (pinned) {
+      if (cudaFreeHost(p) != cudaSuccess) cudaGetLastError();
+    } else {
       std::free(p);
     }
   }

@@ -56,3 +56,32 @@ def test_msv_model_bounds_oracle():
             b = msv_bound(a["msc"], o.m[i], a["msv_tbm"], 512, d)
             ex = np.float32(o.msv(i, d))
             assert b >= ex, (o.m[i], len(d), b, ex)
+
+
+def test_vit_model_bounds_oracle_randomised():
+    """Random profiles across the pre-screen's widths (M 1-512, the edges of
+    every shape included) against random targets that carry degenerate
+    residues and '*', lengths 1-400, and planted homologs: the bound is never
+    below the oracle's Viterbi score."""
+    rng = np.random.default_rng(101)
+    ms = [1, 2, 3, 31, 32, 33, 63, 64, 65, 127, 128, 129, 255, 256, 257, 511, 512]
+    ms += [int(x) for x in rng.integers(4, 512, 8)]
+    profs = [synth.sample_profile(rng, m, f"r{i}") for i, m in enumerate(ms)]
+    o = O.Oracle(text="".join(synth.profile_text(p) for p in profs))
+    alphabet = np.array(list("ACDEFGHIKLMNPQRSTVWYXBZU*"))
+    checked = 0
+    for i in range(o.n):
+        a = o.arrays(i)
+        seqs = []
+        for _ in range(3):
+            L = int(rng.integers(1, 400))
+            seqs.append(O.encode("".join(rng.choice(alphabet, L, p=None))))
+        dom = synth.emit_homolog(rng, profs[i])
+        seqs.append(O.encode(synth.residues_to_str(synth.plant(rng, len(dom) + int(rng.integers(0, 80)), [dom]))))
+        for d in seqs:
+            b = vit_bound(a["msc"], a["t"], o.m[i], d)
+            ex = np.float32(o.viterbi(i, d))
+            assert not np.isnan(b)
+            assert b >= ex, (o.m[i], len(d), b, ex)
+            checked += 1
+    assert checked == 4 * len(ms)

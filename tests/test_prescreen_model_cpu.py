@@ -85,3 +85,26 @@ def test_vit_model_bounds_oracle_randomised():
             assert b >= ex, (o.m[i], len(d), b, ex)
             checked += 1
     assert checked == 4 * len(ms)
+
+
+def test_msv_model_bounds_oracle_randomised():
+    """The MSV pre-screen's bound model against the oracle's f32 MSV on random
+    profiles (M 1-2048), random targets with degenerate residues and '*', and
+    planted homologs, at the narrowest width a lane-group shape gives and at a
+    padded one."""
+    rng = np.random.default_rng(202)
+    ms = [1, 2, 7, 8, 9, 100, 300, 1000, 2048]
+    profs = [synth.sample_profile(rng, m, f"q{i}") for i, m in enumerate(ms)]
+    o = O.Oracle(text="".join(synth.profile_text(p) for p in profs))
+    alphabet = np.array(list("ACDEFGHIKLMNPQRSTVWYXBZU*"))
+    for i in range(o.n):
+        a = o.arrays(i)
+        m = o.m[i]
+        seqs = [O.encode("".join(rng.choice(alphabet, int(rng.integers(1, 300))))) for _ in range(3)]
+        dom = synth.emit_homolog(rng, profs[i])
+        seqs.append(O.encode(synth.residues_to_str(synth.plant(rng, len(dom) + 40, [dom]))))
+        for width in (((m + 7) // 8) * 8, ((m + 63) // 64) * 64 + 64):
+            for d in seqs:
+                b = msv_bound(a["msc"], m, a["msv_tbm"], width, d)
+                ex = np.float32(o.msv(i, d))
+                assert b >= ex, (m, width, len(d), b, ex)
